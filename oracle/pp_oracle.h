@@ -1,0 +1,44 @@
+/*
+ * pp_oracle.h -- CPU restatement of PittPack's single-rank Poisson solve.
+ * TEST INFRASTRUCTURE ONLY (the checker); the product never includes it.
+ */
+#ifndef PP_ORACLE_H
+#define PP_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    PPO_BAD = -1,
+    PPO_DST2 = 0, /* D-D: DST-II forward / DST-III inverse (reference tag 0) */
+    PPO_DCT2 = 1, /* N-N: DCT-II / DCT-III (reference tag 1) */
+    PPO_FFT = 2,  /* P-P: complex DFT (reference tag 2) */
+    PPO_DCT4 = 3, /* N-D: DCT-IV (not in the reference) */
+    PPO_DST4 = 4  /* D-N: DST-IV (not in the reference) */
+};
+
+#define PPO_ERR_INPUT 19 /* the reference's INPUT_ARGS code */
+
+typedef struct {
+    int nx, ny, nz;
+    char bc[6];          /* xmin xmax ymin ymax zmin zmax, letters P N D */
+    double box[6];       /* Xa Xb Ya Yb Za Zb */
+    int compat_zero_mode; /* 1: the reference's zero-mode row replacement */
+    int dirichlet_lift;   /* 1: the reference's modifyRhsDirichlet */
+} ppo_problem;
+
+int ppo_kind_from_bc(char lo, char hi);
+int ppo_check(const ppo_problem* pb);
+double ppo_eigenvalue(const ppo_problem* pb, int kx, int ky);
+void ppo_dft(int n, int sign, double* re, double* im);
+void ppo_dirichlet_lift(const ppo_problem* pb, double* lift);
+/* P: 2*nx*ny*nz doubles, chunkedArray layout P[2*(i+nx*j+nx*ny*k)+{0,1}] */
+int ppo_solve(const ppo_problem* pb, const double* rhs_re, const double* rhs_im, double* P);
+void ppo_manufactured(const ppo_problem* pb, double* f_re, double* f_im, double* u_re, double* u_im);
+void ppo_residual(const ppo_problem* pb, const double* u, const double* b, double* r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,84 @@
+"""The CPU oracle against the reference's golden outputs and against the
+mathematics (7-point residual, manufactured-solution convergence)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+def _load(path):
+    z = np.load(path)
+    bc = str(z["bc"])
+    fi = z["f_im"] if z["f_im"].size else None
+    return int(z["nx"]), int(z["ny"]), int(z["nz"]), bc, tuple(z["box"]), z["f_re"], fi, z["P"]
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_oracle_matches_reference_golden(path):
+    nx, ny, nz, bc, box, fr, fi, P = _load(path)
+    Q = O.solve(O.problem(nx, ny, nz, bc, box), fr, fi)
+    # the oracle restates the reference's arithmetic step by step; the only
+    # foreign piece (the DFT) is the same exactly rounded DFT in both
+    assert O.rel_l2(Q, P) <= 1e-15
+    assert np.max(np.abs(Q - P)) <= 1e-15 * max(1.0, np.max(np.abs(P)))
+
+
+VALID = ["DDDDDD", "NNNNDD", "PPPPDD", "NNDDNN", "DDPPPP", "NDDNDD", "DNPPND", "PPPPPP",
+         "NNNNNN", "DDNNDN", "NDNDNN", "PPPPND"]
+
+
+def _singular(bc):
+    return bc[4] in "NP" and bc[5] in "NP" and bc[0:2] in ("NN", "PP") and bc[2:4] in ("NN", "PP")
+
+
+@pytest.mark.parametrize("bc", VALID)
+@pytest.mark.parametrize("shape", [(12, 10, 9), (7, 9, 5), (16, 8, 4)])
+def test_exact_mode_solves_the_7_point_system(bc, shape):
+    nx, ny, nz = shape
+    rng = np.random.default_rng(hash((bc, shape)) % 2**32)
+    pb = O.problem(nx, ny, nz, bc, compat_zero_mode=0)
+    f = rng.standard_normal((nz, ny, nx))
+    if _singular(bc):
+        f -= f.mean()
+    P = O.solve(pb, f)
+    b = O.scaled_rhs(pb, f)
+    r = O.residual(pb, P.real, b)
+    assert np.linalg.norm(r) <= 1e-13 * np.linalg.norm(b)
+
+
+def test_compat_zero_mode_differs_only_in_the_zero_mode():
+    # NN-NN with Dirichlet z: the reference pins row 0 of the kx=ky=0 column
+    nx, ny, nz = 8, 6, 7
+    f = np.random.default_rng(5).standard_normal((nz, ny, nx))
+    a = O.solve(O.problem(nx, ny, nz, "NNNNDD", compat_zero_mode=1), f)
+    b = O.solve(O.problem(nx, ny, nz, "NNNNDD", compat_zero_mode=0), f)
+    d = (a - b).real
+    # the difference is constant over every z-plane (it lives in kx=ky=0 only)
+    assert np.max(np.abs(d - d.mean(axis=(1, 2), keepdims=True))) < 1e-13
+    assert np.max(np.abs(d)) > 1e-6
+
+
+def test_dft_matches_numpy():
+    rng = np.random.default_rng(0)
+    for n in (2, 3, 5, 8, 12, 30, 97):
+        x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        assert np.allclose(O.dft(x), np.fft.fft(x), rtol=0, atol=1e-13)
+        assert np.allclose(O.dft(x, +1), np.fft.ifft(x) * n, rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("bc", ["NNNNDD", "DDDDDD", "PPPPDD", "DDNNDD"])
+def test_manufactured_solution_converges_second_order(bc):
+    errs = []
+    for n in (8, 16, 32):
+        pb = O.problem(n, n, n, bc)
+        fr, fi, ur, ui = O.manufactured(pb)
+        P = O.solve(pb, fr, fi if bc[0] == "P" else None)
+        e = np.sqrt(np.mean(np.abs(P.real - ur) ** 2 + (np.abs(P.imag - ui) ** 2 if bc[0] == "P" else 0)))
+        errs.append(e)
+    rates = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
+    assert min(rates) > 1.8, (errs, rates)
