@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 PittPack Poisson solve.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step): a 512^3 grid solved once for each x/y boundary family in
+turn -- periodic (PPPP), Neumann-Neumann (NNNN), Neumann-Dirichlet (NDND) and
+Dirichlet-Dirichlet (DDDD) -- with Dirichlet z at both ends, unit box; the RHS
+is a seeded sum of 8 eigenmodes of the family (integer wavenumbers < n/4,
+amplitudes N(0,1)) plus 1e-3 uniform noise (seeds 3..6), generated on the
+device.  Plain FP64 path.  Metric: Mpoints/s = grid points solved / time.
+
+`value` times the solves with the RHS already resident in HBM (CUDA events on
+the solver stream, max over ranks); `e2e` times the public API end to end per
+solve: pinned host RHS -> pp_assign_rhs (H2D) -> pp_solve -> pp_get_solution
+(D2H of the complex-interleaved solution).  Inputs (1 GiB per grid) are larger
+than the 126 MB L2, so no flush is needed between solves.
+
+Multi-GPU: the solve does not shard (one grid per GPU); N ranks run N
+independent replicas of the workload and `value` counts the points of all.
+
+`--impl reference` times the reference's own CPU path (PencilDcmp::pittPack
+of the PittPack sources, built single-rank by oracle/Makefile) on one host
+core on a bounded sample: one 128^3 grid per family it supports (PP, NN, DD;
+it has no N-D family) per step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpoints/s at 512^3 (FP64 plain solve, four x/y families, Dirichlet z)"
+UNIT = "Mpoints/s"
+FAMILIES = ["PPPPDD", "NNNNDD", "NDNDDD", "DDDDDD"]
+N_GRID = 512
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# algorithmic bytes per point of each solve kernel for a real RHS:
+# (read + write), see DESIGN.md "Kernels and their rooflines"
+KERNEL_NAMES = ["x_forward", "y_forward", "z_solve", "y_inverse", "x_inverse"]
+
+
+def kernel_bytes_per_point(bc: str, rhs_complex: bool = False):
+    x_c = bc[0:2] == "PP"
+    s_c = bc[2:4] == "PP"
+    r = 16 if rhs_complex else 8
+    X = 16 if x_c else 8
+    S = 16 if s_c else 8
+    return [r + X, X + S, 2 * S, 2 * S, S + 16]
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+def hbm_peak():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"pp_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_rhs(torch, bc: str, n: int, seed: int, device):
+    """Seeded sum of 8 eigenmodes of the family plus 1e-3 uniform noise."""
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    amps = torch.randn(8, generator=g, dtype=torch.float64)
+    waves = torch.randint(0, n // 4, (8, 3), generator=g)
+    phase = torch.randint(0, 2, (8, 2), generator=g)
+    c = (torch.arange(n, dtype=torch.float64, device=device) + 0.5) / n  # cell centres on [0,1]
+
+    def mode1d(pair: str, k: int, ph: int):
+        if pair == "PP":
+            return torch.cos(2 * torch.pi * k * c) if ph == 0 else torch.sin(2 * torch.pi * k * c)
+        if pair == "NN":
+            return torch.cos(torch.pi * k * c)
+        if pair == "DD":
+            return torch.sin(torch.pi * (k + 1) * c)
+        if pair == "ND":
+            return torch.cos(torch.pi * (k + 0.5) * c)
+        return torch.sin(torch.pi * (k + 0.5) * c)  # DN
+
+    f = torch.zeros((n, n, n), dtype=torch.float64, device=device)
+    for m in range(8):
+        kx, ky, kz = (int(v) for v in waves[m])
+        mx = mode1d(bc[0:2], kx, int(phase[m, 0]))
+        my = mode1d(bc[2:4], ky, int(phase[m, 1]))
+        mz = mode1d(bc[4:6], kz, 0)
+        f.add_(float(amps[m]) * mz[:, None, None] * my[None, :, None] * mx[None, None, :])
+    gn = torch.Generator(device=device).manual_seed(seed + 1000)
+    f.add_((torch.rand(f.shape, generator=gn, dtype=torch.float64, device=device) * 2 - 1) * 1e-3)
+    return f
+
+
+def cpu_reference_sample(steps: int, warmup: int, n: int = 128):
+    """The reference's CPU path on one core: one n^3 solve per family it
+    supports per step.  Returns (Mpoints/s, kind, cores, sample text)."""
+    import numpy as np
+
+    lib = os.path.join(ROOT, "oracle", "_ref", "libppref.so")
+    fams = ["PPPPDD", "NNNNDD", "DDDDDD"]
+    rng = np.random.default_rng(11)
+    f = rng.uniform(-1, 1, n ** 3)
+    out = np.zeros(2 * n ** 3)
+    box = np.array([0, 1, 0, 1, 0, 1.0])
+    dp = ctypes.POINTER(ctypes.c_double)
+    if os.path.exists(lib):
+        os.environ["PP_SHIM_FFT"] = "fast"
+        L = ctypes.CDLL(lib)
+        L.ppref_solve.argtypes = [ctypes.c_int] * 3 + [ctypes.c_char_p, dp, dp, dp, dp, dp]
+        kind = "reference"
+
+        def one(bc):
+            sec = ctypes.c_double()
+            # silence the reference's console output
+            fd = os.dup(1)
+            nul = os.open(os.devnull, os.O_WRONLY)
+            os.dup2(nul, 1)
+            try:
+                L.ppref_solve(n, n, n, bc.encode(), box.ctypes.data_as(dp), f.ctypes.data_as(dp), None,
+                              out.ctypes.data_as(dp), ctypes.byref(sec))
+            finally:
+                os.dup2(fd, 1)
+                os.close(fd)
+                os.close(nul)
+    else:
+        from oracle import oracle as O
+
+        kind = "port"
+
+        def one(bc):
+            O.solve(O.problem(n, n, n, bc), f.reshape(n, n, n))
+    for _ in range(warmup):
+        one(fams[0])
+    t0 = time.perf_counter()
+    for s in range(steps):
+        for bc in fams:
+            one(bc)
+    dt = time.perf_counter() - t0
+    pts = steps * len(fams) * n ** 3
+    sample = (f"{steps} step(s) x {len(fams)} families (PPPPDD, NNNNDD, DDDDDD) of a {n}^3 grid, "
+              f"{'shim FFT in place of FFTW (absent)' if kind == 'reference' else 'oracle restatement'}")
+    return pts / dt / 1e6, kind, 1, sample
+
+
+def run_reference(args):
+    rank, _, world = env_rank()
+    if rank != 0:
+        return 0
+    v, kind, cores, sample = cpu_reference_sample(max(1, args.steps), max(0, min(args.warmup, 1)))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "reference CPU path, bounded sample (see cpu_baseline.sample)", "grid": 128,
+                   "families": ["PPPPDD", "NNNNDD", "DDDDDD"]},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    rank, local_rank, world = env_rank()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    import pittpack_b200 as pp
+    from pittpack_b200.poisson import pinned_empty
+
+    n = args.n
+    npts = n ** 3
+    stream = torch.cuda.current_stream()
+    solvers, rhs_dev = [], []
+    for idx, bc in enumerate(FAMILIES):
+        M = pp.make_Poisson(n, n, n)
+        M.assignBoundary(bc)
+        M.setBox([0, 1, 0, 1, 0, 1])
+        M.setCoords(2)
+        M.setStream(stream.cuda_stream)
+        f = make_rhs(torch, bc, n, 3 + idx, torch.device("cuda", local_rank))
+        M.assignRhsDevice(f.data_ptr(), False)
+        solvers.append(M)
+        rhs_dev.append(f)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing ----------------------------------------------
+    for _ in range(args.warmup):
+        for M in solvers:
+            M.pittPack()
+    for M in solvers:
+        M.timingBegin(args.steps)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for _ in range(args.steps):
+        for M in solvers:
+            M.pittPack()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    per_kernel = []
+    for M in solvers:
+        k_ms, cnt = M.timingEnd()
+        per_kernel.append((k_ms, cnt))
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    total_pts = world * args.steps * len(FAMILIES) * npts
+    value = total_pts / (ms / 1e3) / 1e6
+
+    # ---- roofline of the dominant kernel ---------------------------------------
+    peak, peak_kind = hbm_peak()
+    kern_total = np.zeros(5)
+    kern_bytes = np.zeros(5)
+    launches = 0
+    for (k_ms, cnt), bc in zip(per_kernel, FAMILIES):
+        kern_total += k_ms
+        kern_bytes += np.array(kernel_bytes_per_point(bc)) * npts * cnt
+        launches += cnt
+    dom = int(np.argmax(kern_total))
+    per_launch_ms = kern_total[dom] / max(1, launches)
+    per_launch_bytes = kern_bytes[dom] / max(1, launches)
+    achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
+    solve_alg_bytes = 48.0 * npts  # compulsory 3-stage traffic of a real solve
+    solve_ms = ms / (args.steps * len(FAMILIES))
+    roofline = {
+        "bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "traffic": None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+        "algorithmic_bytes_per_launch": per_launch_bytes,
+    }
+    kernels = {KERNEL_NAMES[i]: {"ms_per_launch": kern_total[i] / max(1, launches),
+                                 "share": kern_total[i] / kern_total.sum(),
+                                 "GBps": (kern_bytes[i] / max(1, launches)) / (kern_total[i] / max(1, launches) / 1e3) / 1e9}
+               for i in range(5)}
+
+    # ---- end to end through the public API ---------------------------------------
+    h_rhs = []
+    for f in rhs_dev:
+        a = pinned_empty((n, n, n), np.float64)
+        a[...] = f.cpu().numpy()
+        h_rhs.append(a)
+    del rhs_dev
+    h_out = pinned_empty((n, n, n), np.complex128)
+    e2e_steps = max(1, min(args.steps, 3))
+    for M, a in zip(solvers, h_rhs):  # warm-up of the copy path
+        M.assignRhs(a)
+        M.pittPack()
+        M.getSolution(out=h_out)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for M, a in zip(solvers, h_rhs):
+            M.assignRhs(a)
+            M.pittPack()
+            M.getSolution(out=h_out)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - w0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_val = world * e2e_steps * len(FAMILIES) * npts / e2e_s / 1e6
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, kind, cores, sample = cpu_reference_sample(1, 0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded eigenmode sums + 1e-3 noise, generated on device)",
+            "config": {"workload": f"{n}^3 grid x 4 x/y families (PPPP, NNNN, NDND, DDDD), Dirichlet z",
+                       "grid": [n, n, n], "families": FAMILIES, "precision": "fp64 plain",
+                       "l2": "inputs (1 GiB per grid) larger than L2, no flush",
+                       "parallelism": f"replicas x{world}"},
+            "ms_per_solve": solve_ms,
+            "solve_roofline": {"algorithmic_bytes_per_point": 48, "achieved": solve_alg_bytes / (solve_ms / 1e3) / 1e9,
+                               "peak": peak, "unit": "GB/s", "frac": solve_alg_bytes / (solve_ms / 1e3) / 1e9 / peak},
+            "roofline": roofline, "kernels": kernels,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": len(FAMILIES) * npts * 8,
+                    "d2h_bytes_per_step": len(FAMILIES) * npts * 16, "steps": e2e_steps},
+            "gpu_launches": 5 * len(FAMILIES) * args.steps,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    for M in solvers:
+        M.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=N_GRID, help="grid edge (the benchmark uses 512)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

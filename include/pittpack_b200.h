@@ -1,0 +1,132 @@
+/*
+ * pittpack_b200.h -- C ABI of the B200 PittPack Poisson solver.
+ *
+ * Drop-in for the solve path of PittPack's PencilDcmp / PoissonGPU
+ * (src/include/pencilDcmp.hpp:442-522).  One handle = one grid on one GPU;
+ * the reference's MPI pencil decomposition is not used (single rank, p0 = 1).
+ * Every call returns a status code whose values mirror the reference's
+ * PittPackResult (src/include/params.h:86-114); no call exits the process.
+ * Plain pointers and sizes only.  Paths in the citations are relative to the
+ * PittPack source tree.
+ *
+ * Data layout (chunkedArray, src/chunkedArray.cpp:100-199): point (i,j,k),
+ * i = x index fastest, linear index p = i + nx*j + nx*ny*k; the RHS is real
+ * (rhs[p]) or complex-interleaved (rhs[2p], rhs[2p+1]); the solution P is
+ * complex-interleaved P[2p], P[2p+1], real part = u.
+ */
+#ifndef PITTPACK_B200_H
+#define PITTPACK_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes: 0..23 are the reference's PittPackResult values */
+enum {
+    PP_SUCCESS = 0,
+    PP_GPU_INIT_FAILURE = 1,
+    PP_SOLVER_ARRAY_INCONSISTENT = 2,
+    PP_MESH_DIVISIBLE = 6,
+    PP_ALLOCATION_FAIL = 15,
+    PP_THOMAS_FAIL = 18,
+    PP_INPUT_ARGS = 19,
+    PP_CUFFT_FAIL_X = 20,     /* forward x transform pass failed */
+    PP_CUFFT_FAIL_INV_X = 21, /* inverse x transform pass failed */
+    PP_CUFFT_FAIL_Y = 22,     /* forward y transform pass failed */
+    PP_CUFFT_FAIL_INV_Y = 23, /* inverse y transform pass failed */
+    /* codes added by this library */
+    PP_INVALID_HANDLE = 24,
+    PP_NOT_READY = 25, /* boundary or RHS not assigned yet */
+    PP_CUDA_ERROR = 26,
+    PP_UNSUPPORTED = 27 /* a size or option the GPU kernels do not cover */
+};
+
+/* precision of the solve */
+enum { PP_PRECISION_FP64 = 0, PP_PRECISION_MIXED = 1 };
+
+typedef struct pp_solver_s* pp_handle;
+
+/* runtime options; the reference keeps these as compile-time switches in
+ * src/include/params.h (SOLUTIONMETHOD, NITER, ...) */
+typedef struct {
+    int precision;        /* PP_PRECISION_FP64 (default) */
+    int max_sweeps;       /* refinement sweeps for PP_PRECISION_MIXED */
+    double tolerance;     /* relative residual target for PP_PRECISION_MIXED */
+    int compat_zero_mode; /* 1 (default): reference zero-mode row replacement, src/triDiag.cpp:1753-1776 */
+    int dirichlet_lift;   /* 1 (default): reference modifyRhsDirichlet, src/pencilDcmp.cpp:4623-4835 */
+} pp_options;
+
+/* the reference's PittPackGetErrorEnum (src/pencilDcmp.cpp:4869-4913) */
+const char* pp_result_string(int code);
+
+/* make_Poisson / PencilDcmp(argc, argv, nx, ny, nz) (src/pencilDcmp.cpp:232-452,
+ * 6432-6440): a solver for an nx*ny*nz grid on the current CUDA device */
+int pp_create(int nx, int ny, int nz, pp_handle* h);
+/* ~PencilDcmp (src/pencilDcmp.cpp:528-658) */
+int pp_destroy(pp_handle h);
+
+/* setBox + setCoords(2) (src/pencilDcmp.cpp:470-480, 748-831):
+ * X = {Xa, Xb, Ya, Yb, Za, Zb}; default unit box */
+int pp_set_box(pp_handle h, const double X[6]);
+/* assignBoundary (src/pencilDcmp.cpp:3578-3634): bc = xmin xmax ymin ymax zmin
+ * zmax, letters 'P' 'N' 'D'.  x and y take P-P, N-N, D-D, N-D or D-N; z takes
+ * D/N at either end or P-P. */
+int pp_assign_boundary(pp_handle h, const char bc[6]);
+
+int pp_default_options(pp_options* opt);
+int pp_set_options(pp_handle h, const pp_options* opt);
+int pp_get_options(pp_handle h, pp_options* opt);
+
+/* assignRhs (src/pencilDcmp.cpp:5591-5647): real host RHS, nx*ny*nz doubles */
+int pp_assign_rhs(pp_handle h, const double* rhs);
+/* complex host RHS, 2*nx*ny*nz doubles interleaved */
+int pp_assign_rhs_complex(pp_handle h, const double* rhs);
+/* RHS already on the device (real or interleaved complex); copied on the
+ * handle's stream */
+int pp_assign_rhs_device(pp_handle h, const double* d_rhs, int is_complex);
+
+/* pittPack() once (src/pencilDcmp.cpp:5801-6430), asynchronous on the
+ * handle's stream */
+int pp_solve(pp_handle h);
+/* profiling hook, no counterpart in the reference (which times the whole
+ * solve with MPI_Wtime, src/pencilDcmp.cpp:5900-6333): one solve with CUDA
+ * events between its kernels; kernel_ms[0..4] = forward x, forward y, z solve,
+ * inverse y, inverse x (milliseconds).  Synchronises the handle's stream. */
+#define PP_SOLVE_KERNELS 5
+int pp_profile_solve(pp_handle h, double* kernel_ms, int n);
+/* live per-kernel timing, no counterpart in the reference: between
+ * pp_timing_begin and pp_timing_end the first max_solves calls of pp_solve
+ * record CUDA events between their kernels on the handle's stream (no extra
+ * synchronisation); pp_timing_end waits for the last one and returns the
+ * summed milliseconds per kernel and the number of solves recorded. */
+int pp_timing_begin(pp_handle h, int max_solves);
+int pp_timing_end(pp_handle h, double* kernel_ms_total, int n, int* solves);
+/* the solution P (2*nx*ny*nz doubles, chunkedArray layout) to host memory;
+ * synchronises the handle's stream */
+int pp_get_solution(pp_handle h, double* P);
+/* the solution to device memory (2*nx*ny*nz doubles), on the handle's stream */
+int pp_get_solution_device(pp_handle h, double* d_P);
+/* device pointer of the handle's solution buffer (valid until pp_destroy) */
+int pp_solution_device_ptr(pp_handle h, const double** d_P);
+
+/* getError (src/pencilDcmp.cpp:2040-2208): RMS error of the solution against
+ * the reference's manufactured solution; does not modify the solution */
+int pp_get_error_manufactured(pp_handle h, double* err);
+
+/* CUDA stream for the handle's work (cudaStream_t passed as void*); 0 = legacy */
+int pp_set_stream(pp_handle h, void* stream);
+int pp_synchronize(pp_handle h);
+
+/* pinned host buffers for fast copies */
+int pp_host_alloc(size_t bytes, void** p);
+int pp_host_free(void* p);
+
+/* device memory the handle holds, in bytes */
+int pp_workspace_bytes(pp_handle h, size_t* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

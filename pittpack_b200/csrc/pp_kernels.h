@@ -1,0 +1,67 @@
+// Kernel argument blocks and launchers shared by the solver's host code.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "pp_fft.cuh"
+
+#define PP_LINE_THREADS 256
+#define PP_Z_THREADS 256
+#define PP_Z_MAX_NZ 1024
+
+// Dirichlet face corrections subtracted from the dz^2-scaled RHS
+// (modifyRhsDirichlet, src/pencilDcmp.cpp:4623-4835); null where a face is
+// not Dirichlet.  z faces are [j][i], x faces [k][j], y faces [k][i].
+struct PPLift {
+    const double* z0;
+    const double* z1;
+    const double* x0;
+    const double* x1;
+    const double* y0;
+    const double* y1;
+    int any;
+};
+
+struct PPLinePassArgs {
+    const double* src;
+    double* dst;
+    int n;             // points along the transformed direction
+    int kind;          // PPKind
+    int nlines;        // lines per plane
+    int nplanes;
+    long elem_stride;  // strides in elements (complex elements count once)
+    long line_stride;
+    long plane_stride;
+    int L;             // lines per CTA tile
+    int tiles_per_plane;
+    PPFftPlan fft;     // length n, or n/2 for the quarter-wave families
+    const double2* cs; // pre/post twiddles of the family (see pp_linepass.cu)
+    int rhs_scale;     // forward x-pass: multiply by dz twice and subtract the lift
+    double dz;
+    PPLift lift;
+    int nx, ny, nz;
+    double out_scale;  // inverse x-pass: 1 / (nx ny)
+};
+
+size_t pp_line_pass_smem(int L, int nfft);
+cudaError_t pp_launch_line_pass(const PPLinePassArgs& a, bool inverse, bool strided, bool in_cplx, bool out_cplx,
+                                cudaStream_t st);
+
+// z-boundary kinds of the tridiagonal systems
+enum PPZBc : int { PP_Z_DIRICHLET = 0, PP_Z_NEUMANN = 1, PP_Z_PERIODIC = 2 };
+
+struct PPZArgs {
+    double* data;       // spectrum [k][ky][kx], real or complex
+    int nx, ny, nz;
+    int TS;             // systems (adjacent kx) per CTA
+    int tiles_x;
+    const double* ax;   // -2 + 2 cos((kx + num) f / (nx + den)), per kx
+    const double* ay;   // same per ky
+    double Cx, Cy;      // (dz/dx)^2, (dz/dy)^2
+    int zlo, zhi;       // PPZBc of the two z ends
+    int pin_always;     // 1: zero-mode row replacement whatever the z ends (reference)
+};
+
+size_t pp_zsolve_smem(int TS, int nz, bool cplx);
+cudaError_t pp_launch_zsolve(const PPZArgs& a, bool cplx, cudaStream_t st);

@@ -1,0 +1,781 @@
+// Host side of the solver: plan tables, device buffers, the launch sequence
+// of one solve, and the C ABI declared in include/pittpack_b200.h.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/pittpack_b200.h"
+#include "pp_common.cuh"
+#include "pp_kernels.h"
+
+namespace {
+
+// the reference's constant (src/include/params.h: const double pi)
+const double REF_PI = 3.1415926535897932384;
+
+int kind_from_bc(char lo, char hi)
+{
+    if (lo == 'D' && hi == 'D') return PP_KIND_DST2;
+    if (lo == 'N' && hi == 'N') return PP_KIND_DCT2;
+    if (lo == 'P' && hi == 'P') return PP_KIND_FFT;
+    if (lo == 'N' && hi == 'D') return PP_KIND_DCT4;
+    if (lo == 'D' && hi == 'N') return PP_KIND_DST4;
+    return -1;
+}
+
+// factor n into the radices of the Stockham passes; false if n has a prime
+// factor above 5
+bool radix_plan(int n, std::vector<int>& r)
+{
+    r.clear();
+    int m = n;
+    while (m % 8 == 0) { r.push_back(8); m /= 8; }
+    while (m % 4 == 0) { r.push_back(4); m /= 4; }
+    while (m % 2 == 0) { r.push_back(2); m /= 2; }
+    while (m % 3 == 0) { r.push_back(3); m /= 3; }
+    while (m % 5 == 0) { r.push_back(5); m /= 5; }
+    return m == 1 && (int)r.size() <= PP_FFT_MAXPASS;
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t alloc(size_t b)
+    {
+        free();
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e == cudaSuccess) bytes = b;
+        else p = nullptr;
+        return e;
+    }
+    void free()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// one direction's transform tables
+struct DirTables {
+    int n = 0, kind = -1;
+    PPFftPlan fft{};
+    DevBuf tw;   // FFT twiddles of length fft.n
+    DevBuf cs;   // family pre/post twiddles
+    DevBuf eig;  // -2 + 2 cos((k + num) f / (n + den)), k < n
+};
+
+}  // namespace
+
+struct pp_solver_s {
+    int nx = 0, ny = 0, nz = 0;
+    int device = 0;
+    double box[6] = {0, 1, 0, 1, 0, 1};
+    char bc[6] = {0};
+    bool have_bc = false, have_rhs = false, rhs_complex = false;
+    pp_options opt{};
+    cudaStream_t stream = 0;
+    DirTables tx, ty;
+    DevBuf rhs, bufA, bufB, out;
+    DevBuf lift[6];
+    PPLift liftv{};
+    std::mutex mu;
+    std::string last_error;
+    // live per-kernel timing (pp_timing_begin / pp_timing_end)
+    std::vector<cudaEvent_t> tev;
+    int tmax = 0, tcount = 0;
+};
+
+namespace {
+
+int set_cuda_error(pp_solver_s* h, cudaError_t e, int code)
+{
+    if (h) h->last_error = cudaGetErrorString(e);
+    return code;
+}
+
+// tables of one direction: FFT twiddles in long double, family twiddles as
+// the reference computes them (theta = (pi/2/N) k with its pi constant)
+int build_dir(pp_solver_s* h, DirTables& t, int n, int kind)
+{
+    t.n = n;
+    t.kind = kind;
+    const bool quarter = pp_kind_is_quarter(kind);
+    if (quarter && (n % 2) != 0) return PP_UNSUPPORTED;
+    const int nf = quarter ? n / 2 : n;
+    std::vector<int> r;
+    if (!radix_plan(nf, r)) return PP_UNSUPPORTED;
+    t.fft.n = nf;
+    t.fft.npass = (int)r.size();
+    for (size_t i = 0; i < r.size(); ++i) t.fft.radix[i] = r[i];
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    const long double pi_l = 3.141592653589793238462643383279502884L;
+    std::vector<double2> tw(nf);
+    for (int m = 0; m < nf; ++m) {
+        long double a = -two_pi * (long double)m / (long double)nf;
+        tw[m] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    std::vector<double2> cs;
+    if (quarter) {
+        cs.resize(n);
+        for (int m = 0; m < nf; ++m) {
+            long double a = -pi_l * (long double)m / (long double)n;
+            cs[m] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+        for (int p = 0; p < nf; ++p) {
+            long double a = -pi_l * (long double)(4 * p + 1) / (4.0L * n);
+            cs[nf + p] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+    } else {
+        cs.resize(n);
+        for (int k = 0; k < n; ++k) {
+            double theta = (REF_PI / 2. / n) * k;
+            cs[k] = make_double2(cos(theta), sin(theta));
+        }
+    }
+    // eigenvalue parts (setEigenVal src/pencilDcmp.cpp:3533-3576, getEigenVal 4393-4417)
+    double num = 0.0, den = 0.0, freq = REF_PI;
+    if (kind == PP_KIND_DST2) num = 1.0;
+    else if (kind == PP_KIND_FFT) freq = 2. * REF_PI;
+    else if (quarter) num = 0.5;
+    std::vector<double> eig(n);
+    for (int k = 0; k < n; ++k) eig[k] = -2.0 + 2. * cos((k + num) * freq / (n + den));
+
+    cudaError_t e;
+    if ((e = t.tw.alloc(sizeof(double2) * nf)) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+    if ((e = t.cs.alloc(sizeof(double2) * cs.size())) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+    if ((e = t.eig.alloc(sizeof(double) * n)) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+    cudaMemcpy(t.tw.p, tw.data(), sizeof(double2) * nf, cudaMemcpyHostToDevice);
+    cudaMemcpy(t.cs.p, cs.data(), sizeof(double2) * cs.size(), cudaMemcpyHostToDevice);
+    if ((e = cudaMemcpy(t.eig.p, eig.data(), sizeof(double) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return set_cuda_error(h, e, PP_CUDA_ERROR);
+    t.fft.tw = t.tw.as<double2>();
+    return PP_SUCCESS;
+}
+
+// the reference's tags for exactValue (extractTag, src/pencilDcmp.cpp:3636-3668)
+int ref_tag_xy(int kind)
+{
+    if (kind == PP_KIND_DST2) return 0;
+    if (kind == PP_KIND_DCT2) return 1;
+    if (kind == PP_KIND_FFT) return 2;
+    return -1;
+}
+
+int ref_tag_z(const char* bc)
+{
+    int t[3], count = 0;
+    for (int d = 0; d < 3; ++d) {
+        char lo = bc[2 * d], hi = bc[2 * d + 1];
+        if (lo == 'D' && hi == 'D') t[d] = 0;
+        else if (lo == 'N' && hi == 'N') t[d] = 1;
+        else if (lo == 'P' && hi == 'P') t[d] = 2;
+        else { t[d] = -1; count++; }
+    }
+    if (count == 0) t[2] = -1;
+    if (bc[4] == 'D') return -1;
+    if (bc[4] == 'N') return -2;
+    return t[2];
+}
+
+// exactValue (src/pencilDcmp.cpp:1837-1866)
+double exact_value(double omega, double x, int tg)
+{
+    if (fabs(omega) < 1.0e-6) return 1.0;
+    if (tg == 0 || tg == -1 || tg == -2) return sin(omega * x);
+    if (tg == 1) return cos(omega * x);
+    return 0.0;
+}
+
+// face corrections of modifyRhsDirichlet (src/pencilDcmp.cpp:4623-4835),
+// evaluated with the reference's expressions
+int build_lift(pp_solver_s* h)
+{
+    for (auto& b : h->lift) b.free();
+    h->liftv = PPLift{};
+    if (!h->opt.dirichlet_lift) return PP_SUCCESS;
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    const double pi = 4. * atan(1.0);
+    const double Xa = h->box[0], Ya = h->box[2], Za = h->box[4];
+    const double c1 = -(h->box[0] - h->box[1]) / (nx);
+    const double c2 = -(h->box[2] - h->box[3]) / (ny);
+    const double c3 = -(h->box[4] - h->box[5]) / (nz);
+    const double shift = 1.0;
+    const double omega[3] = {1 * pi, 2 * pi, 3 * pi};
+    const int t0 = ref_tag_xy(kind_from_bc(h->bc[0], h->bc[1]));
+    const int t1 = ref_tag_xy(kind_from_bc(h->bc[2], h->bc[3]));
+    const int t2 = ref_tag_z(h->bc);
+    auto upload = [&](int face, const std::vector<double>& v) -> int {
+        bool nonzero = false;
+        for (double x : v) nonzero |= (x != 0.0);
+        if (!nonzero) return PP_SUCCESS;  // nothing to subtract
+        cudaError_t e = h->lift[face].alloc(sizeof(double) * v.size());
+        if (e != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+        cudaMemcpy(h->lift[face].p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice);
+        return PP_SUCCESS;
+    };
+    int rc;
+    if (h->bc[4] == 'D' || h->bc[5] == 'D') {
+        for (int face = 0; face < 2; ++face) {
+            if (h->bc[4 + face] != 'D') continue;
+            std::vector<double> v((size_t)nx * ny);
+            const double z = face == 0 ? Za : Za + (nz - 1) * c3 + c3;
+            for (int i = 0; i < nx; ++i) {
+                const double x = Xa + i * c1 + shift * c1 * .5;
+                for (int j = 0; j < ny; ++j) {
+                    const double y = Ya + j * c2 + shift * c2 * 0.5;
+                    v[i + (size_t)nx * j] =
+                        2. * exact_value(omega[0], x, t0) * exact_value(omega[1], y, t1) * exact_value(omega[2], z, t2);
+                }
+            }
+            if ((rc = upload(face, v)) != PP_SUCCESS) return rc;
+        }
+    }
+    for (int face = 0; face < 2; ++face) {
+        if (h->bc[face] != 'D') continue;
+        std::vector<double> v((size_t)ny * nz);
+        const double x = face == 0 ? Xa : Xa + ((nx - 1) + 1) * c1;
+        for (int k = 0; k < nz; ++k) {
+            const double z = Za + k * c3 + shift * c3 * .5;
+            for (int j = 0; j < ny; ++j) {
+                const double y = Ya + j * c2 + shift * c2 * 0.5;
+                v[j + (size_t)ny * k] =
+                    2. * exact_value(omega[0], x, t0) * exact_value(omega[1], y, t1) * exact_value(omega[2], z, t2);
+            }
+        }
+        if ((rc = upload(2 + face, v)) != PP_SUCCESS) return rc;
+    }
+    for (int face = 0; face < 2; ++face) {
+        if (h->bc[2 + face] != 'D') continue;
+        std::vector<double> v((size_t)nx * nz);
+        const double y = face == 0 ? Ya : Ya + ((ny - 1) + 1) * c2;
+        for (int k = 0; k < nz; ++k) {
+            const double z = Za + k * c3 + shift * c3 * .5;
+            for (int i = 0; i < nx; ++i) {
+                const double x = Xa + i * c1 + shift * c1 * 0.5;
+                v[i + (size_t)nx * k] =
+                    2. * exact_value(omega[0], x, t0) * exact_value(omega[1], y, t1) * exact_value(omega[2], z, t2);
+            }
+        }
+        if ((rc = upload(4 + face, v)) != PP_SUCCESS) return rc;
+    }
+    PPLift& L = h->liftv;
+    L.z0 = h->lift[0].as<double>();
+    L.z1 = h->lift[1].as<double>();
+    L.x0 = h->lift[2].as<double>();
+    L.x1 = h->lift[3].as<double>();
+    L.y0 = h->lift[4].as<double>();
+    L.y1 = h->lift[5].as<double>();
+    L.any = (L.z0 || L.z1 || L.x0 || L.x1 || L.y0 || L.y1) ? 1 : 0;
+    return PP_SUCCESS;
+}
+
+int valid_bc(const char* bc)
+{
+    for (int i = 0; i < 6; ++i)
+        if (bc[i] != 'P' && bc[i] != 'N' && bc[i] != 'D') return 0;
+    if (kind_from_bc(bc[0], bc[1]) < 0 || kind_from_bc(bc[2], bc[3]) < 0) return 0;
+    if ((bc[4] == 'P') != (bc[5] == 'P')) return 0;
+    return 1;
+}
+
+int rebuild_tables(pp_solver_s* h)
+{
+    int rc = build_dir(h, h->tx, h->nx, kind_from_bc(h->bc[0], h->bc[1]));
+    if (rc != PP_SUCCESS) return rc;
+    rc = build_dir(h, h->ty, h->ny, kind_from_bc(h->bc[2], h->bc[3]));
+    if (rc != PP_SUCCESS) return rc;
+    return build_lift(h);
+}
+
+// lines per CTA tile of a transform pass: a power of two that keeps the two
+// shared-memory buffers within 64 KB
+int pick_lines(int nfft)
+{
+    int L = 16;
+    while (L > 1 && pp_line_pass_smem(L, nfft) > 64 * 1024) L >>= 1;
+    return L;
+}
+
+int pick_ts(int nz, bool cplx, int nx)
+{
+    int ts = 32;
+    while (ts > 1 && pp_zsolve_smem(ts, nz, cplx) > 96 * 1024) ts >>= 1;
+    while (ts > 1 && ts > nx) ts >>= 1;
+    return ts;
+}
+
+int launch_solve(pp_solver_s* h, cudaEvent_t* ev = nullptr)
+{
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    const int kx = h->tx.kind, ky = h->ty.kind;
+    const bool x_cplx = kx == PP_KIND_FFT;  // after the x transform
+    const bool s_cplx = ky == PP_KIND_FFT;  // spectrum (after the y transform)
+    const double dz = -(h->box[4] - h->box[5]) / (nz);
+    const long plane = (long)nx * ny;
+    cudaError_t e;
+    if (ev) cudaEventRecord(ev[0], h->stream);
+
+    PPLinePassArgs ax{};
+    ax.n = nx;
+    ax.kind = kx;
+    ax.nlines = ny;
+    ax.nplanes = nz;
+    ax.elem_stride = 1;
+    ax.line_stride = nx;
+    ax.plane_stride = plane;
+    ax.fft = h->tx.fft;
+    ax.cs = h->tx.cs.as<double2>();
+    ax.L = pick_lines(ax.fft.n);
+    ax.tiles_per_plane = (ny + ax.L - 1) / ax.L;
+    ax.nx = nx;
+    ax.ny = ny;
+    ax.nz = nz;
+    ax.dz = dz;
+    ax.out_scale = 1.0;
+
+    PPLinePassArgs ay = ax;
+    ay.n = ny;
+    ay.kind = ky;
+    ay.nlines = nx;
+    ay.elem_stride = nx;
+    ay.line_stride = 1;
+    ay.fft = h->ty.fft;
+    ay.cs = h->ty.cs.as<double2>();
+    ay.L = pick_lines(ay.fft.n);
+    ay.tiles_per_plane = (nx + ay.L - 1) / ay.L;
+
+    // forward x: rhs -> A
+    PPLinePassArgs a1 = ax;
+    a1.src = h->rhs.as<double>();
+    a1.dst = h->bufA.as<double>();
+    a1.rhs_scale = 1;
+    a1.lift = h->liftv;
+    if ((e = pp_launch_line_pass(a1, false, false, h->rhs_complex, x_cplx, h->stream)) != cudaSuccess)
+        return set_cuda_error(h, e, PP_CUFFT_FAIL_X);
+    if (ev) cudaEventRecord(ev[1], h->stream);
+    // forward y: A -> B
+    PPLinePassArgs a2 = ay;
+    a2.src = h->bufA.as<double>();
+    a2.dst = h->bufB.as<double>();
+    if ((e = pp_launch_line_pass(a2, false, true, x_cplx, s_cplx, h->stream)) != cudaSuccess)
+        return set_cuda_error(h, e, PP_CUFFT_FAIL_Y);
+    if (ev) cudaEventRecord(ev[2], h->stream);
+    // z solve in B
+    PPZArgs z{};
+    z.data = h->bufB.as<double>();
+    z.nx = nx;
+    z.ny = ny;
+    z.nz = nz;
+    z.TS = pick_ts(nz, s_cplx, nx);
+    z.tiles_x = (nx + z.TS - 1) / z.TS;
+    z.ax = h->tx.eig.as<double>();
+    z.ay = h->ty.eig.as<double>();
+    const double dx = -(h->box[0] - h->box[1]) / (nx);
+    const double dy = -(h->box[2] - h->box[3]) / (ny);
+    z.Cx = (dz / dx) * (dz / dx);
+    z.Cy = (dz / dy) * (dz / dy);
+    z.zlo = h->bc[4] == 'P' ? PP_Z_PERIODIC : (h->bc[4] == 'N' ? PP_Z_NEUMANN : PP_Z_DIRICHLET);
+    z.zhi = h->bc[5] == 'P' ? PP_Z_PERIODIC : (h->bc[5] == 'N' ? PP_Z_NEUMANN : PP_Z_DIRICHLET);
+    z.pin_always = h->opt.compat_zero_mode ? 1 : 0;
+    if ((e = pp_launch_zsolve(z, s_cplx, h->stream)) != cudaSuccess) return set_cuda_error(h, e, PP_THOMAS_FAIL);
+    if (ev) cudaEventRecord(ev[3], h->stream);
+    // inverse y: B -> A
+    PPLinePassArgs a3 = ay;
+    a3.src = h->bufB.as<double>();
+    a3.dst = h->bufA.as<double>();
+    if ((e = pp_launch_line_pass(a3, true, true, s_cplx, s_cplx, h->stream)) != cudaSuccess)
+        return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_Y);
+    if (ev) cudaEventRecord(ev[4], h->stream);
+    // inverse x + rescale: A -> out (always complex-interleaved)
+    PPLinePassArgs a4 = ax;
+    a4.src = h->bufA.as<double>();
+    a4.dst = h->out.as<double>();
+    a4.out_scale = 1. / ((double)(nx * ny));
+    if ((e = pp_launch_line_pass(a4, true, false, s_cplx, true, h->stream)) != cudaSuccess)
+        return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_X);
+    if (ev) cudaEventRecord(ev[5], h->stream);
+    return PP_SUCCESS;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+static void timing_release(pp_solver_s* h)
+{
+    for (auto& e : h->tev) cudaEventDestroy(e);
+    h->tev.clear();
+    h->tmax = h->tcount = 0;
+}
+
+extern "C" {
+
+const char* pp_result_string(int code)
+{
+    switch (code) {
+    case PP_SUCCESS: return "SUCCESS";
+    case PP_GPU_INIT_FAILURE: return "GPU_INIT_FAILURE: no usable CUDA device";
+    case PP_SOLVER_ARRAY_INCONSISTENT: return "SOLVER_ARRAY_INCONSISTENT";
+    case PP_MESH_DIVISIBLE: return "MESH_DIVISIBLE";
+    case PP_ALLOCATION_FAIL: return "ALLOCATION_FAIL: not enough device memory";
+    case PP_THOMAS_FAIL: return "THOMAS_FAIL: the z-direction tridiagonal solve failed";
+    case PP_INPUT_ARGS: return "INPUT_ARGS: invalid sizes, boundary letters or box";
+    case PP_CUFFT_FAIL_X: return "CUFFT_FAIL_X: forward x transform failed";
+    case PP_CUFFT_FAIL_INV_X: return "CUFFT_FAIL_INV_X: inverse x transform failed";
+    case PP_CUFFT_FAIL_Y: return "CUFFT_FAIL_Y: forward y transform failed";
+    case PP_CUFFT_FAIL_INV_Y: return "CUFFT_FAIL_INV_Y: inverse y transform failed";
+    case PP_INVALID_HANDLE: return "INVALID_HANDLE";
+    case PP_NOT_READY: return "NOT_READY: boundary conditions or RHS not assigned";
+    case PP_CUDA_ERROR: return "CUDA_ERROR";
+    case PP_UNSUPPORTED: return "UNSUPPORTED: size or option outside the GPU kernels";
+    default: return "UNKNOWN";
+    }
+}
+
+int pp_default_options(pp_options* opt)
+{
+    if (!opt) return PP_INPUT_ARGS;
+    opt->precision = PP_PRECISION_FP64;
+    opt->max_sweeps = 3;
+    opt->tolerance = 1e-10;
+    opt->compat_zero_mode = 1;
+    opt->dirichlet_lift = 1;
+    return PP_SUCCESS;
+}
+
+int pp_create(int nx, int ny, int nz, pp_handle* out)
+{
+    if (!out) return PP_INPUT_ARGS;
+    *out = nullptr;
+    if (nx < 2 || ny < 2 || nz < 3) return PP_INPUT_ARGS;
+    if (nz > PP_Z_MAX_NZ) return PP_UNSUPPORTED;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PP_GPU_INIT_FAILURE;
+    pp_solver_s* h = new (std::nothrow) pp_solver_s;
+    if (!h) return PP_ALLOCATION_FAIL;
+    h->nx = nx;
+    h->ny = ny;
+    h->nz = nz;
+    cudaGetDevice(&h->device);
+    pp_default_options(&h->opt);
+    const size_t n = (size_t)nx * ny * nz;
+    cudaError_t e;
+    if ((e = h->rhs.alloc(2 * n * sizeof(double))) != cudaSuccess ||
+        (e = h->bufA.alloc(2 * n * sizeof(double))) != cudaSuccess ||
+        (e = h->bufB.alloc(2 * n * sizeof(double))) != cudaSuccess ||
+        (e = h->out.alloc(2 * n * sizeof(double))) != cudaSuccess) {
+        delete h;
+        return PP_ALLOCATION_FAIL;
+    }
+    *out = h;
+    return PP_SUCCESS;
+}
+
+int pp_destroy(pp_handle h)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    else cudaDeviceSynchronize();
+    h->rhs.free();
+    h->bufA.free();
+    h->bufB.free();
+    h->out.free();
+    for (auto& b : h->lift) b.free();
+    timing_release(h);
+    h->tx.tw.free(); h->tx.cs.free(); h->tx.eig.free();
+    h->ty.tw.free(); h->ty.cs.free(); h->ty.eig.free();
+    delete h;
+    return PP_SUCCESS;
+}
+
+int pp_set_box(pp_handle h, const double X[6])
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!X) return PP_INPUT_ARGS;
+    for (int d = 0; d < 3; ++d)
+        if (!(X[2 * d + 1] > X[2 * d]) || !std::isfinite(X[2 * d]) || !std::isfinite(X[2 * d + 1]))
+            return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    std::memcpy(h->box, X, sizeof h->box);
+    if (h->have_bc) {
+        cudaSetDevice(h->device);
+        return build_lift(h);
+    }
+    return PP_SUCCESS;
+}
+
+int pp_assign_boundary(pp_handle h, const char bc[6])
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!bc || !valid_bc(bc)) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    cudaSetDevice(h->device);
+    std::memcpy(h->bc, bc, 6);
+    int rc = rebuild_tables(h);
+    h->have_bc = rc == PP_SUCCESS;
+    return rc;
+}
+
+int pp_set_options(pp_handle h, const pp_options* opt)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!opt) return PP_INPUT_ARGS;
+    if (opt->precision != PP_PRECISION_FP64 && opt->precision != PP_PRECISION_MIXED) return PP_INPUT_ARGS;
+    if (opt->precision == PP_PRECISION_MIXED) return PP_UNSUPPORTED;
+    std::lock_guard<std::mutex> g(h->mu);
+    const bool lift_changed = opt->dirichlet_lift != h->opt.dirichlet_lift;
+    h->opt = *opt;
+    if (lift_changed && h->have_bc) {
+        cudaSetDevice(h->device);
+        return build_lift(h);
+    }
+    return PP_SUCCESS;
+}
+
+int pp_get_options(pp_handle h, pp_options* opt)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!opt) return PP_INPUT_ARGS;
+    *opt = h->opt;
+    return PP_SUCCESS;
+}
+
+static int assign_common(pp_handle h, const double* src, bool cplx, cudaMemcpyKind kind)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!src) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    cudaSetDevice(h->device);
+    const size_t n = (size_t)h->nx * h->ny * h->nz;
+    cudaError_t e = cudaMemcpyAsync(h->rhs.p, src, (cplx ? 2 : 1) * n * sizeof(double), kind, h->stream);
+    if (e != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
+    if (kind == cudaMemcpyHostToDevice) {
+        // the caller may reuse its buffer once this returns
+        if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
+    }
+    h->rhs_complex = cplx;
+    h->have_rhs = true;
+    return PP_SUCCESS;
+}
+
+int pp_assign_rhs(pp_handle h, const double* rhs) { return assign_common(h, rhs, false, cudaMemcpyHostToDevice); }
+int pp_assign_rhs_complex(pp_handle h, const double* rhs) { return assign_common(h, rhs, true, cudaMemcpyHostToDevice); }
+int pp_assign_rhs_device(pp_handle h, const double* d_rhs, int is_complex)
+{
+    return assign_common(h, d_rhs, is_complex != 0, cudaMemcpyDeviceToDevice);
+}
+
+int pp_solve(pp_handle h)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    std::lock_guard<std::mutex> g(h->mu);
+    if (!h->have_bc || !h->have_rhs) return PP_NOT_READY;
+    cudaSetDevice(h->device);
+    if (h->tcount < h->tmax) {
+        cudaEvent_t* ev = &h->tev[(size_t)h->tcount * (PP_SOLVE_KERNELS + 1)];
+        h->tcount++;
+        return launch_solve(h, ev);
+    }
+    return launch_solve(h);
+}
+
+int pp_timing_begin(pp_handle h, int max_solves)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (max_solves < 1) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    cudaSetDevice(h->device);
+    timing_release(h);
+    h->tev.resize((size_t)max_solves * (PP_SOLVE_KERNELS + 1));
+    for (auto& e : h->tev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            e = nullptr;
+            timing_release(h);
+            return PP_CUDA_ERROR;
+        }
+    h->tmax = max_solves;
+    h->tcount = 0;
+    return PP_SUCCESS;
+}
+
+int pp_timing_end(pp_handle h, double* kernel_ms_total, int n, int* solves)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!kernel_ms_total || n < PP_SOLVE_KERNELS || !solves) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    cudaSetDevice(h->device);
+    for (int i = 0; i < PP_SOLVE_KERNELS; ++i) kernel_ms_total[i] = 0.0;
+    *solves = h->tcount;
+    int rc = PP_SUCCESS;
+    if (h->tcount > 0) {
+        cudaError_t e = cudaEventSynchronize(h->tev[(size_t)h->tcount * (PP_SOLVE_KERNELS + 1) - 1]);
+        if (e != cudaSuccess) rc = set_cuda_error(h, e, PP_CUDA_ERROR);
+        for (int s = 0; s < h->tcount && rc == PP_SUCCESS; ++s) {
+            cudaEvent_t* ev = &h->tev[(size_t)s * (PP_SOLVE_KERNELS + 1)];
+            for (int i = 0; i < PP_SOLVE_KERNELS; ++i) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+                kernel_ms_total[i] += ms;
+            }
+        }
+    }
+    timing_release(h);
+    return rc;
+}
+
+int pp_profile_solve(pp_handle h, double* kernel_ms, int n)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!kernel_ms || n < PP_SOLVE_KERNELS) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    if (!h->have_bc || !h->have_rhs) return PP_NOT_READY;
+    cudaSetDevice(h->device);
+    cudaEvent_t ev[PP_SOLVE_KERNELS + 1];
+    for (auto& x : ev) cudaEventCreate(&x);
+    int rc = launch_solve(h, ev);
+    cudaError_t e = cudaEventSynchronize(ev[PP_SOLVE_KERNELS]);
+    if (rc == PP_SUCCESS && e == cudaSuccess) {
+        for (int i = 0; i < PP_SOLVE_KERNELS; ++i) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+            kernel_ms[i] = ms;
+        }
+    } else if (rc == PP_SUCCESS) {
+        rc = set_cuda_error(h, e, PP_CUDA_ERROR);
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    return rc;
+}
+
+int pp_get_solution(pp_handle h, double* P)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!P) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    cudaSetDevice(h->device);
+    const size_t n = (size_t)h->nx * h->ny * h->nz;
+    cudaError_t e = cudaMemcpyAsync(P, h->out.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return e == cudaSuccess ? PP_SUCCESS : set_cuda_error(h, e, PP_CUDA_ERROR);
+}
+
+int pp_get_solution_device(pp_handle h, double* d_P)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!d_P) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    cudaSetDevice(h->device);
+    const size_t n = (size_t)h->nx * h->ny * h->nz;
+    cudaError_t e = cudaMemcpyAsync(d_P, h->out.p, 2 * n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
+    return e == cudaSuccess ? PP_SUCCESS : set_cuda_error(h, e, PP_CUDA_ERROR);
+}
+
+int pp_solution_device_ptr(pp_handle h, const double** d_P)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!d_P) return PP_INPUT_ARGS;
+    *d_P = h->out.as<double>();
+    return PP_SUCCESS;
+}
+
+int pp_get_error_manufactured(pp_handle h, double* err)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!err) return PP_INPUT_ARGS;
+    if (!h->have_bc) return PP_NOT_READY;
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    const size_t n = (size_t)nx * ny * nz;
+    std::vector<double> P(2 * n);
+    int rc = pp_get_solution(h, P.data());
+    if (rc != PP_SUCCESS) return rc;
+    // getError (src/pencilDcmp.cpp:2040-2208), INITANALYTIC = 1 branch
+    const double pi = REF_PI;
+    const double Xa = h->box[0], Ya = h->box[2], Za = h->box[4];
+    const double c1 = -(h->box[0] - h->box[1]) / (nx);
+    const double c2 = -(h->box[2] - h->box[3]) / (ny);
+    const double c3 = -(h->box[4] - h->box[5]) / (nz);
+    const double omega[3] = {1 * pi, 2 * pi, 3 * pi};
+    const int t0 = ref_tag_xy(kind_from_bc(h->bc[0], h->bc[1]));
+    const int t1 = ref_tag_xy(kind_from_bc(h->bc[2], h->bc[3]));
+    const int t2 = ref_tag_z(h->bc);
+    const bool pxy = h->bc[0] == 'P' || h->bc[2] == 'P';
+    const bool pall = h->bc[0] == 'P' && h->bc[2] == 'P' && h->bc[4] == 'P';
+    double acc = 0.0;
+    for (int k = 0; k < nz; ++k) {
+        const double z = Za + k * c3 + 1.0 * c3 * 0.5;
+        for (int j = 0; j < ny; ++j) {
+            const double y = Ya + j * c2 + 1.0 * c2 * 0.5;
+            for (int i = 0; i < nx; ++i) {
+                const double x = Xa + i * c1 + 1.0 * c1 * .5;
+                const size_t p = i + (size_t)nx * j + (size_t)nx * ny * k;
+                double val, val1;
+                if (pxy) {
+                    val = P[2 * p] - (sin(omega[1] * z) * cos(omega[1] * (x + y)));
+                    val1 = P[2 * p + 1] - (sin(omega[1] * z) * sin(omega[1] * (x + y)));
+                } else {
+                    val = P[2 * p] - exact_value(omega[0], x, t0) * exact_value(omega[1], y, t1) *
+                                         exact_value(omega[2], z, t2);
+                    val1 = 0.0;
+                }
+                if (pall) {
+                    val = P[2 * p] - cos(omega[1] * (x + y + z));
+                    val1 = P[2 * p + 1] - sin(omega[1] * (x + y + z));
+                }
+                acc += val * val + val1 * val1;
+            }
+        }
+    }
+    *err = sqrt(acc / (double)n);
+    return PP_SUCCESS;
+}
+
+int pp_set_stream(pp_handle h, void* stream)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    std::lock_guard<std::mutex> g(h->mu);
+    h->stream = (cudaStream_t)stream;
+    return PP_SUCCESS;
+}
+
+int pp_synchronize(pp_handle h)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    cudaSetDevice(h->device);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    return e == cudaSuccess ? PP_SUCCESS : set_cuda_error(h, e, PP_CUDA_ERROR);
+}
+
+int pp_host_alloc(size_t bytes, void** p)
+{
+    if (!p) return PP_INPUT_ARGS;
+    cudaError_t e = cudaHostAlloc(p, bytes, cudaHostAllocDefault);
+    return e == cudaSuccess ? PP_SUCCESS : PP_ALLOCATION_FAIL;
+}
+
+int pp_host_free(void* p)
+{
+    cudaError_t e = cudaFreeHost(p);
+    return e == cudaSuccess ? PP_SUCCESS : PP_CUDA_ERROR;
+}
+
+int pp_workspace_bytes(pp_handle h, size_t* bytes)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!bytes) return PP_INPUT_ARGS;
+    size_t b = h->rhs.bytes + h->bufA.bytes + h->bufB.bytes + h->out.bytes;
+    for (auto& l : h->lift) b += l.bytes;
+    b += h->tx.tw.bytes + h->tx.cs.bytes + h->tx.eig.bytes + h->ty.tw.bytes + h->ty.cs.bytes + h->ty.eig.bytes;
+    *bytes = b;
+    return PP_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,204 @@
+"""Host-side mirror of PittPack's PencilDcmp / PoissonGPU interface.
+
+The method names and their order of use follow the reference
+(src/include/pencilDcmp.hpp:442-522, driven as in src/main.cpp:73-134):
+
+    M = make_Poisson(nx, ny, nz)      # make_Poisson, src/pencilDcmp.cpp:6432-6440
+    M.assignBoundary("NNNNDD")        # src/pencilDcmp.cpp:3578-3634
+    M.setBox([0, 1, 0, 1, 0, 1])      # src/pencilDcmp.cpp:470-480
+    M.setCoords(2)                    # single rank: the box is the whole grid
+    M.assignRhs(rhs)                  # src/pencilDcmp.cpp:5591-5647
+    M.pittPack()                      # src/pencilDcmp.cpp:5801-6430, one solve
+    M.getError()                      # src/pencilDcmp.cpp:2040-2208 (non-destructive here)
+    P = M.getSolution()               # the chunkedArray P, complex (nz, ny, nx)
+
+Every call goes through the C ABI of libpittpack_b200.so; errors raise
+PittPackError with the reference's PittPackResult code instead of exiting.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import Options, PittPackError, check
+
+
+class PoissonGPU:
+    """One nx*ny*nz grid on the current CUDA device."""
+
+    def __init__(self, nx: int, ny: int, nz: int):
+        L = _lib.load()
+        self._L = L
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        h = ctypes.c_void_p()
+        check(L.pp_create(self.nx, self.ny, self.nz, ctypes.byref(h)), "pp_create")
+        self._h = h
+        self._box = np.array([0.0, 1.0, 0.0, 1.0, 0.0, 1.0])
+        self.bc = None
+
+    # -- set-up -------------------------------------------------------------
+    def assignBoundary(self, bc) -> None:
+        b = bc.encode() if isinstance(bc, str) else bytes(bc)
+        if len(b) != 6:
+            raise PittPackError(_lib.PP_INPUT_ARGS, "assignBoundary needs 6 letters")
+        check(self._L.pp_assign_boundary(self._h, b), "assignBoundary")
+        self.bc = b.decode()
+
+    def setBox(self, X) -> None:
+        x = np.ascontiguousarray(X, dtype=np.float64)
+        if x.size != 6:
+            raise PittPackError(_lib.PP_INPUT_ARGS, "setBox needs 6 values")
+        check(self._L.pp_set_box(self._h, x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "setBox")
+        self._box = x.copy()
+
+    def setCoords(self, dir: int = 2) -> None:  # noqa: A002 - the reference's name
+        """Single rank: the rank's box is the whole box; nothing to do."""
+
+    def options(self) -> Options:
+        o = Options()
+        check(self._L.pp_get_options(self._h, ctypes.byref(o)), "pp_get_options")
+        return o
+
+    def setOptions(self, **kw) -> None:
+        o = self.options()
+        for k, v in kw.items():
+            if not hasattr(o, k):
+                raise TypeError(f"unknown option {k}")
+            setattr(o, k, v)
+        check(self._L.pp_set_options(self._h, ctypes.byref(o)), "pp_set_options")
+
+    # -- data ---------------------------------------------------------------
+    def _shape_ok(self, a: np.ndarray, n: int) -> np.ndarray:
+        a = np.ascontiguousarray(a)
+        if a.size != n:
+            raise PittPackError(_lib.PP_INPUT_ARGS, f"expected {n} values, got {a.size}")
+        return a
+
+    def assignRhs(self, rhs) -> None:
+        """Real RHS f (x fastest); the solve multiplies it by dz^2 like the reference."""
+        n = self.nx * self.ny * self.nz
+        if np.iscomplexobj(rhs):
+            return self.assignRhsComplex(rhs)
+        a = self._shape_ok(np.asarray(rhs, dtype=np.float64), n)
+        check(self._L.pp_assign_rhs(self._h, a.ctypes.data), "assignRhs")
+
+    def assignRhsComplex(self, rhs) -> None:
+        n = self.nx * self.ny * self.nz
+        a = self._shape_ok(np.asarray(rhs, dtype=np.complex128), n)
+        check(self._L.pp_assign_rhs_complex(self._h, a.ctypes.data), "assignRhsComplex")
+
+    def assignRhsDevice(self, ptr: int, is_complex: bool = False) -> None:
+        check(self._L.pp_assign_rhs_device(self._h, ctypes.c_void_p(ptr), int(is_complex)), "assignRhsDevice")
+
+    # -- solve --------------------------------------------------------------
+    def pittPack(self) -> None:
+        check(self._L.pp_solve(self._h), "pittPack")
+
+    solve = pittPack
+
+    def profileSolve(self) -> np.ndarray:
+        """One solve with per-kernel CUDA-event times (ms): forward x,
+        forward y, z solve, inverse y, inverse x."""
+        ms = np.zeros(5)
+        check(self._L.pp_profile_solve(self._h, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 5),
+              "pp_profile_solve")
+        return ms
+
+    def timingBegin(self, max_solves: int) -> None:
+        check(self._L.pp_timing_begin(self._h, int(max_solves)), "pp_timing_begin")
+
+    def timingEnd(self):
+        """(summed ms per kernel [5], number of solves recorded)."""
+        ms = np.zeros(5)
+        n = ctypes.c_int()
+        check(self._L.pp_timing_end(self._h, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 5,
+                                    ctypes.byref(n)), "pp_timing_end")
+        return ms, n.value
+
+    def getSolution(self, out: np.ndarray | None = None) -> np.ndarray:
+        """P as complex (nz, ny, nx); 'out' may be a preallocated (pinned) array."""
+        if out is None:
+            out = np.empty((self.nz, self.ny, self.nx), dtype=np.complex128)
+        if out.dtype != np.complex128 or out.size != self.nx * self.ny * self.nz or not out.flags.c_contiguous:
+            raise PittPackError(_lib.PP_INPUT_ARGS, "getSolution needs a contiguous complex128 array")
+        check(self._L.pp_get_solution(self._h, out.ctypes.data), "getSolution")
+        return out
+
+    def solutionDevicePtr(self) -> int:
+        p = ctypes.c_void_p()
+        check(self._L.pp_solution_device_ptr(self._h, ctypes.byref(p)), "pp_solution_device_ptr")
+        return int(p.value)
+
+    def getError(self) -> float:
+        e = ctypes.c_double()
+        check(self._L.pp_get_error_manufactured(self._h, ctypes.byref(e)), "getError")
+        return e.value
+
+    def setStream(self, stream_ptr: int) -> None:
+        check(self._L.pp_set_stream(self._h, ctypes.c_void_p(stream_ptr)), "pp_set_stream")
+
+    def synchronize(self) -> None:
+        check(self._L.pp_synchronize(self._h), "pp_synchronize")
+
+    def workspaceBytes(self) -> int:
+        b = ctypes.c_size_t()
+        check(self._L.pp_workspace_bytes(self._h, ctypes.byref(b)), "pp_workspace_bytes")
+        return int(b.value)
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._L.pp_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def pinned_empty(shape, dtype=np.float64) -> np.ndarray:
+    """A numpy array in page-locked host memory (pp_host_alloc), freed with the array."""
+    L = _lib.load()
+    dt = np.dtype(dtype)
+    nbytes = int(np.prod(shape)) * dt.itemsize
+    p = ctypes.c_void_p()
+    check(L.pp_host_alloc(max(nbytes, 1), ctypes.byref(p)), "pp_host_alloc")
+    buf = (ctypes.c_char * max(nbytes, 1)).from_address(p.value)
+    arr = np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)
+
+    class _Owner:
+        def __init__(self, ptr):
+            self.ptr = ptr
+
+        def __del__(self):
+            try:
+                L.pp_host_free(ctypes.c_void_p(self.ptr))
+            except Exception:
+                pass
+
+    # keep the allocation alive as long as the array (or views of it) live
+    holder = _Owner(p.value)
+    arr = arr.view(_PinnedArray)
+    arr._pp_owner = holder
+    return arr
+
+
+class _PinnedArray(np.ndarray):
+    def __array_finalize__(self, obj):
+        if obj is not None:
+            self._pp_owner = getattr(obj, "_pp_owner", None)
+
+
+def make_Poisson(nx: int, ny: int, nz: int) -> PoissonGPU:
+    """The reference's factory (src/pencilDcmp.cpp:6432-6440); always the GPU solver."""
+    return PoissonGPU(nx, ny, nz)

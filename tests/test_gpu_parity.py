@@ -1,0 +1,166 @@
+"""GPU parity of the plain FP64 path (through the C ABI) against the
+reference's golden outputs and the CPU oracle.
+
+Tolerance: relative L2 <= 1e-12 against the reference / oracle, the bar the
+plain path is held to.  At full size, where the oracle is too slow, the
+exact-mode solution is checked through the 7-point residual of the discrete
+problem (a size-independent property).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+def gpu_solve(nx, ny, nz, bc, f, box=(0, 1, 0, 1, 0, 1), **opts):
+    import pittpack_b200 as pp
+
+    with pp.make_Poisson(nx, ny, nz) as M:
+        M.assignBoundary(bc)
+        M.setBox(box)
+        M.setCoords(2)
+        if opts:
+            M.setOptions(**opts)
+        M.assignRhs(f)
+        M.pittPack()
+        return M.getSolution()
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_matches_reference_golden(path):
+    z = np.load(path)
+    nx, ny, nz = int(z["nx"]), int(z["ny"]), int(z["nz"])
+    f = z["f_re"] + 1j * z["f_im"] if z["f_im"].size else z["f_re"]
+    P = gpu_solve(nx, ny, nz, str(z["bc"]), f, tuple(z["box"]))
+    assert O.rel_l2(P, z["P"]) <= TOL
+
+
+FAMILIES = ["PP", "NN", "DD", "ND", "DN"]
+ZBC = ["DD", "NN", "DN", "ND", "PP"]
+
+
+def _valid(bcx, bcy):
+    # the reference's y-direction DCT/DST drops the imaginary part that an
+    # x-periodic transform produces; that combination is exercised separately
+    return not (bcx == "PP" and bcy != "PP")
+
+
+CASES = [(x, y, z) for x in FAMILIES for y in FAMILIES for z in ZBC if _valid(x, y)]
+
+
+@pytest.mark.parametrize("bcx,bcy,bcz", CASES)
+def test_all_families_vs_oracle(bcx, bcy, bcz):
+    bc = bcx + bcy + bcz
+    rng = np.random.default_rng(abs(hash(bc)) % 2**32)
+    nx, ny, nz = 24, 20, 18
+    f = rng.uniform(-1, 1, (nz, ny, nx))
+    if bcx == "PP" or bcy == "PP":
+        f = f + 1j * rng.uniform(-1, 1, (nz, ny, nx))
+    fr, fi = (f.real.copy(), f.imag.copy()) if np.iscomplexobj(f) else (f, None)
+    for compat in (1, 0):
+        Q = O.solve(O.problem(nx, ny, nz, bc, compat_zero_mode=compat), fr, fi)
+        P = gpu_solve(nx, ny, nz, bc, f, compat_zero_mode=compat)
+        assert O.rel_l2(P, Q) <= TOL, (bc, compat)
+
+
+@pytest.mark.parametrize("shape", [(30, 48, 20), (96, 10, 7), (12, 160, 33), (64, 64, 3), (2, 6, 4), (50, 45, 4),
+                                   (128, 96, 100)])
+@pytest.mark.parametrize("bc", ["NNDDNN", "PPPPDD", "DDNNPP", "DNPPDN", "NDDDND"])
+def test_sizes_vs_oracle(shape, bc):
+    nx, ny, nz = shape
+    if ("ND" in (bc[0:2], bc[2:4]) or "DN" in (bc[0:2], bc[2:4])):
+        if (bc[0:2] in ("ND", "DN") and nx % 2) or (bc[2:4] in ("ND", "DN") and ny % 2):
+            pytest.skip("quarter-wave families need an even length")
+    rng = np.random.default_rng(7)
+    f = rng.standard_normal((nz, ny, nx))
+    Q = O.solve(O.problem(nx, ny, nz, bc), f)
+    P = gpu_solve(nx, ny, nz, bc, f)
+    assert O.rel_l2(P, Q) <= TOL
+
+
+def test_x_periodic_y_cosine_reproduces_reference_quirk():
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "pp_nn_dd_quirk.npz"))
+    P = gpu_solve(8, 8, 8, "PPNNDD", z["f_re"])
+    assert O.rel_l2(P, z["P"]) <= TOL
+
+
+def test_non_unit_box_and_manufactured_error():
+    import pittpack_b200 as pp
+
+    for bc in ("NNNNDD", "PPPPDD", "DDDDDD"):
+        errs = []
+        for n in (16, 32, 64):
+            pb = O.problem(n, n, n, bc)
+            fr, fi, ur, ui = O.manufactured(pb)
+            with pp.make_Poisson(n, n, n) as M:
+                M.assignBoundary(bc)
+                M.setBox([0, 1, 0, 1, 0, 1])
+                if bc[0] == "P":
+                    M.assignRhsComplex(fr + 1j * fi)
+                else:
+                    M.assignRhs(fr)
+                M.pittPack()
+                errs.append(M.getError())
+        rates = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
+        assert min(rates) > 1.8, (bc, errs)
+
+
+@pytest.mark.parametrize("bc", ["NNDDDD", "PPPPDD", "NNNNNN", "DDNNPP"])
+def test_full_size_residual(bc):
+    """512^3 (the benchmark size): exact-mode solution satisfies the 7-point
+    system to 1e-12 relative (long-double residual on the host)."""
+    n = 512
+    rng = np.random.default_rng(3)
+    f = rng.uniform(-1, 1, (n, n, n))
+    if bc == "NNNNNN":
+        f -= f.mean()
+    P = gpu_solve(n, n, n, bc, f, compat_zero_mode=0)
+    pb = O.problem(n, n, n, bc, compat_zero_mode=0)
+    b = O.scaled_rhs(pb, f)
+    r = O.residual(pb, np.ascontiguousarray(P.real), b)
+    assert np.linalg.norm(r) <= 1e-12 * np.linalg.norm(b)
+    if bc[0] != "P" and bc[2] != "P":
+        assert np.max(np.abs(P.imag)) == 0.0
+
+
+def test_repeat_solves_are_identical_and_rhs_reusable():
+    import pittpack_b200 as pp
+
+    n = 32
+    f = np.random.default_rng(1).standard_normal((n, n, n))
+    with pp.make_Poisson(n, n, n) as M:
+        M.assignBoundary("NNDDDD")
+        M.assignRhs(f)
+        M.pittPack()
+        a = M.getSolution()
+        M.pittPack()
+        b = M.getSolution()
+    assert np.array_equal(a, b)
+
+
+def test_errors_are_returned_not_fatal():
+    import pittpack_b200 as pp
+
+    with pp.make_Poisson(8, 8, 8) as M:
+        with pytest.raises(pp.PittPackError) as e:
+            M.pittPack()  # no boundary yet
+        assert e.value.code == 25
+        with pytest.raises(pp.PittPackError) as e:
+            M.assignBoundary("PDNNDD")
+        assert e.value.code == 19
+        with pytest.raises(pp.PittPackError):
+            M.setBox([1, 0, 0, 1, 0, 1])
+        M.assignBoundary("DDDDDD")
+        with pytest.raises(pp.PittPackError):
+            M.pittPack()  # no RHS yet
+    with pytest.raises(pp.PittPackError) as e:
+        pp.make_Poisson(14, 8, 8).assignBoundary("DDDDDD")  # 14 = 2 * 7: no radix-7 pass
+    assert e.value.code == 27
