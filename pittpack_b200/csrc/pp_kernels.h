@@ -8,7 +8,7 @@
 
 #define PP_LINE_THREADS 256
 #define PP_Z_THREADS 256
-#define PP_Z_MAX_NZ 1024
+#define PP_Z_MAX_NZ 4096
 
 // Dirichlet face corrections subtracted from the dz^2-scaled RHS
 // (modifyRhsDirichlet, src/pencilDcmp.cpp:4623-4835); null where a face is
@@ -42,9 +42,19 @@ struct PPLinePassArgs {
     PPLift lift;
     int nx, ny, nz;
     double out_scale;  // inverse x-pass: 1 / (nx ny)
+    // used by the power-of-two kernel (pp_linepass_pow2.cu)
+    const void* tw;    // FFT twiddles (double2 or float2), length n or n/2
+    const void* cs2;   // family twiddles in the kernel's precision
+    int in_cplx, out_cplx;
 };
 
 size_t pp_line_pass_smem(int L, int nfft);
+// power-of-two lengths 16..2048: complex FFT lines per CTA (0 = not covered);
+// a tile holds this many data lines for the periodic family and twice as many
+// for the real families
+int pp_lp2_lpc(int n);
+template <typename Real, typename TI, typename TO>
+cudaError_t pp_launch_line_pass_pow2(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st);
 cudaError_t pp_launch_line_pass(const PPLinePassArgs& a, bool inverse, bool strided, bool in_cplx, bool out_cplx,
                                 cudaStream_t st);
 
@@ -61,7 +71,13 @@ struct PPZArgs {
     double Cx, Cy;      // (dz/dx)^2, (dz/dy)^2
     int zlo, zhi;       // PPZBc of the two z ends
     int pin_always;     // 1: zero-mode row replacement whatever the z ends (reference)
+    int P;              // lanes per system (set by the launcher)
 };
+
+// lanes that share one z system (a power of two <= 32)
+int pp_zsolve_lanes(int nz, bool cplx);
+// systems per CTA and threads per CTA of the z solve
+void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads);
 
 size_t pp_zsolve_smem(int TS, int nz, bool cplx);
 cudaError_t pp_launch_zsolve(const PPZArgs& a, bool cplx, cudaStream_t st);

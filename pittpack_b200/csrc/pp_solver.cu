@@ -2,6 +2,7 @@
 // of one solve, and the C ABI declared in include/pittpack_b200.h.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -303,12 +304,23 @@ int pick_lines(int nfft)
     return L;
 }
 
-int pick_ts(int nz, bool cplx, int nx)
+// one transform pass: the register-resident kernel for power-of-two lengths,
+// the generic shared-memory Stockham kernel otherwise
+cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool strided, bool in_cplx,
+                      bool out_cplx, cudaStream_t st)
 {
-    int ts = 32;
-    while (ts > 1 && pp_zsolve_smem(ts, nz, cplx) > 96 * 1024) ts >>= 1;
-    while (ts > 1 && ts > nx) ts >>= 1;
-    return ts;
+    const int lpc = pp_lp2_lpc(d.n);
+    if (lpc > 0) {
+        a.tw = d.tw.p;
+        a.cs2 = d.cs.p;
+        a.in_cplx = in_cplx;
+        a.out_cplx = out_cplx;
+        const int dl = d.kind == PP_KIND_FFT ? lpc : 2 * lpc;
+        a.L = dl;
+        a.tiles_per_plane = (a.nlines + dl - 1) / dl;
+        return pp_launch_line_pass_pow2<double, double, double>(a, inverse, strided, st);
+    }
+    return pp_launch_line_pass(a, inverse, strided, in_cplx, out_cplx, st);
 }
 
 int launch_solve(pp_solver_s* h, cudaEvent_t* ev = nullptr)
@@ -357,14 +369,14 @@ int launch_solve(pp_solver_s* h, cudaEvent_t* ev = nullptr)
     a1.dst = h->bufA.as<double>();
     a1.rhs_scale = 1;
     a1.lift = h->liftv;
-    if ((e = pp_launch_line_pass(a1, false, false, h->rhs_complex, x_cplx, h->stream)) != cudaSuccess)
+    if ((e = line_pass(a1, h->tx, false, false, h->rhs_complex, x_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_X);
     if (ev) cudaEventRecord(ev[1], h->stream);
     // forward y: A -> B
     PPLinePassArgs a2 = ay;
     a2.src = h->bufA.as<double>();
     a2.dst = h->bufB.as<double>();
-    if ((e = pp_launch_line_pass(a2, false, true, x_cplx, s_cplx, h->stream)) != cudaSuccess)
+    if ((e = line_pass(a2, h->ty, false, true, x_cplx, s_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_Y);
     if (ev) cudaEventRecord(ev[2], h->stream);
     // z solve in B
@@ -373,7 +385,8 @@ int launch_solve(pp_solver_s* h, cudaEvent_t* ev = nullptr)
     z.nx = nx;
     z.ny = ny;
     z.nz = nz;
-    z.TS = pick_ts(nz, s_cplx, nx);
+    int zthreads = 0;
+    pp_zsolve_config(nz, s_cplx, nx, &z.TS, &zthreads);
     z.tiles_x = (nx + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
     z.ay = h->ty.eig.as<double>();
@@ -390,7 +403,7 @@ int launch_solve(pp_solver_s* h, cudaEvent_t* ev = nullptr)
     PPLinePassArgs a3 = ay;
     a3.src = h->bufB.as<double>();
     a3.dst = h->bufA.as<double>();
-    if ((e = pp_launch_line_pass(a3, true, true, s_cplx, s_cplx, h->stream)) != cudaSuccess)
+    if ((e = line_pass(a3, h->ty, true, true, s_cplx, s_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_Y);
     if (ev) cudaEventRecord(ev[4], h->stream);
     // inverse x + rescale: A -> out (always complex-interleaved)
@@ -398,7 +411,7 @@ int launch_solve(pp_solver_s* h, cudaEvent_t* ev = nullptr)
     a4.src = h->bufA.as<double>();
     a4.dst = h->out.as<double>();
     a4.out_scale = 1. / ((double)(nx * ny));
-    if ((e = pp_launch_line_pass(a4, true, false, s_cplx, true, h->stream)) != cudaSuccess)
+    if ((e = line_pass(a4, h->tx, true, false, s_cplx, true, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_X);
     if (ev) cudaEventRecord(ev[5], h->stream);
     return PP_SUCCESS;

@@ -1,4 +1,4 @@
-// Batched z-direction tridiagonal solve, one system per warp.
+// Batched z-direction tridiagonal solve.
 //
 // The reference gathers each strided z-line into a buffer and runs a serial
 // Thomas sweep per line (solveThmBatch, src/pencilDcmp.cpp:5066-5105 ->
@@ -18,14 +18,18 @@
 //   * a CTA owns TS adjacent kx columns of one ky row; it reads the TS x nz
 //     tile with coalesced row segments into shared memory (rows skewed by one
 //     slot every 16 to spread banks), solves, and writes the tile back;
-//   * each warp solves one system at a time by the partition method: lane L
-//     owns a contiguous block of M ~ nz/32 rows, eliminates it to express
-//     every interior unknown through the block's first and last unknown
-//     (forward sweep + backward sweep, one division per row), which leaves two
-//     equations per lane.  The 2P-row reduced tridiagonal system is solved by
-//     parallel cyclic reduction in shared memory; periodic systems apply
-//     Sherman-Morrison on the reduced system.  Each lane then recovers its
-//     interior rows from its two solved end values.
+//   * a group of P lanes (P = 32 / systems per warp) solves one system by the
+//     partition method: lane L owns a contiguous block of M ~ nz/P rows and
+//     eliminates it so that every interior unknown is expressed through the
+//     block's first and last unknown (forward sweep with one division per
+//     row, then a backward sweep), leaving two equations per lane.  Interior
+//     rows have the same coefficients in every block, so the pivots and
+//     spikes of a block depend only on lambda; the group's lane 0 records them
+//     in a shared table that the other lanes read in the backward sweep and
+//     the recovery, so no lane keeps per-row arrays in registers;
+//   * the 2P-row reduced system is solved by parallel cyclic reduction in
+//     shared memory; periodic systems apply Sherman-Morrison to the reduced
+//     system; each lane then recovers its interior rows.
 #include <type_traits>
 
 #include "pp_common.cuh"
@@ -50,24 +54,51 @@ PP_D double2 zzero<double2>() { return make_double2(0.0, 0.0); }
 PP_HD int zpos(int k) { return k + (k >> 4); }
 PP_HD int zpitch(int nz) { return (zpos(nz - 1) + 1) | 1; }
 
-constexpr int RED_ROWS = 64;
+// shared-memory layout of one CTA
+struct ZLayout {
+    int pitch;       // tile column pitch (elements)
+    int mmax;        // table rows per group
+    int groups;      // groups (systems in flight) per CTA
+    int P;           // lanes per system
+    size_t tile_off, tab_off, red_off, bytes;
+};
 
-template <bool CPLX, int MMAX>
+PP_HD ZLayout zlayout(int TS, int nz, int P, bool cplx, int nthreads)
+{
+    ZLayout L;
+    const size_t e = cplx ? 16 : 8;
+    L.P = P;
+    L.pitch = zpitch(nz);
+    L.mmax = (nz + P - 1) / P + 1;
+    L.groups = nthreads / P;
+    L.tile_off = 0;
+    L.tab_off = (size_t)TS * L.pitch * e;
+    L.tab_off = (L.tab_off + 15) & ~(size_t)15;
+    L.red_off = L.tab_off + (size_t)L.groups * L.mmax * 16;
+    // per group: 2P rows of a, c, u (doubles) and d (element)
+    L.bytes = L.red_off + (size_t)L.groups * 2 * P * (24 + e);
+    return L;
+}
+
+template <bool CPLX>
 __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
 {
     using T = typename std::conditional<CPLX, double2, double>::type;
-    extern __shared__ double zsm[];
+    extern __shared__ __align__(16) unsigned char zsm_raw[];
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const int pitch = zpitch(nz);
-    T* tile = reinterpret_cast<T*>(zsm);
-    const int nwarps = blockDim.x >> 5;
-    const int warp = threadIdx.x >> 5;
-    const int lane = threadIdx.x & 31;
-    double* red = zsm + (size_t)a.TS * pitch * (CPLX ? 2 : 1);
-    double* ra = red + (size_t)warp * RED_ROWS * (CPLX ? 5 : 4);
-    double* rc = ra + RED_ROWS;
-    double* ru = rc + RED_ROWS;
-    T* rd = reinterpret_cast<T*>(ru + RED_ROWS);
+    const int P = a.P;
+    const ZLayout Lz = zlayout(a.TS, nz, P, CPLX, blockDim.x);
+    T* tile = reinterpret_cast<T*>(zsm_raw + Lz.tile_off);
+
+    const int group = threadIdx.x / P;
+    const int lane = threadIdx.x - group * P;
+    double2* tab = reinterpret_cast<double2*>(zsm_raw + Lz.tab_off) + (size_t)group * Lz.mmax;  // (p_i, alpha_i)
+    const int m = 2 * P;
+    unsigned char* redb = zsm_raw + Lz.red_off + (size_t)group * m * (24 + sizeof(T));
+    double* ra = reinterpret_cast<double*>(redb);
+    double* rc = ra + m;
+    double* ru = rc + m;
+    T* rd = reinterpret_cast<T*>(ru + m);
 
     const int ky = blockIdx.x / a.tiles_x;
     const int kx0 = (blockIdx.x - ky * a.tiles_x) * a.TS;
@@ -79,28 +110,30 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     for (int idx = threadIdx.x; idx < ts * nz; idx += blockDim.x) {
         const int k = idx / ts;
         const int s = idx - k * ts;
-        tile[s * pitch + zpos(k)] = g[k * plane + col0 + s];
+        tile[s * Lz.pitch + zpos(k)] = g[k * plane + col0 + s];
     }
     __syncthreads();
 
-    const int P = min(32, nz / 2);
     const int bsz = nz / P;
     const int rem = nz - bsz * P;
-    const bool active = lane < P;
-    const int M = active ? bsz + (lane < rem ? 1 : 0) : 0;
+    const int M = bsz + (lane < rem ? 1 : 0);
     const int s0 = lane * bsz + min(lane, rem);
-    const int m = 2 * P;
     const bool periodic = a.zlo == PP_Z_PERIODIC;
     const bool has_d = a.zlo == PP_Z_DIRICHLET || a.zhi == PP_Z_DIRICHLET;
+    const unsigned full = 0xffffffffu;
 
-    for (int s = warp; s < ts; s += nwarps) {
-        const int kx = kx0 + s;
+    // all groups of a warp run the same number of iterations (warp-synchronous steps)
+    const int ngroups = Lz.groups;
+    const int iters = (a.TS + ngroups - 1) / ngroups;
+    for (int it = 0; it < iters; ++it) {
+        const int s = group + it * ngroups;
+        const bool live = s < ts;
+        const int kx = kx0 + (live ? s : 0);
         const double lam = (-2.0 + a.ax[kx] * a.Cx) + a.ay[ky] * a.Cy;
         const bool zero = fabs(lam + 2.) < 1.e-10;
         const bool pin = zero && (periodic || a.pin_always || !has_d);
-        T* col = tile + s * pitch;
+        T* col = tile + (live ? s : 0) * Lz.pitch;
 
-        // coefficients of the first and last rows
         double A0, B0, C0, AN, BN, CN;
         if (periodic) {
             A0 = 1.0;
@@ -118,78 +151,67 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             CN = 0.0;
         }
 
-        // ---- local elimination of the lane's block ----------------------------
-        // alpha (coefficient of the block's first unknown) and gamma (of the
-        // next unknown) stay in registers; delta overwrites the RHS in the
-        // tile column, which only this lane touches for these rows.
-        double al[MMAX], ga[MMAX];
-        double rA0 = 0, rB0 = 1, rC0 = 0;
-        T rD0 = zzero<T>();
-        double e1a = 0, e1c = 0;
-        T e1d = zzero<T>();
-        T dprev = zzero<T>();
-#pragma unroll
-        for (int i = 0; i < MMAX; ++i) {
-            if (i < M) {
+        // ---- forward sweep of the lane's block -------------------------------------
+        // row i (i >= 1) becomes alpha_i x_0 + x_i + gamma_i x_{i+1} = delta_i; delta
+        // overwrites the RHS in the tile (only this lane touches these rows)
+        double rA0 = 1.0, rB0 = lam, rC0 = 1.0;
+        if (s0 == 0) {
+            rA0 = A0;
+            rB0 = B0;
+            rC0 = C0;
+        }
+        T rD0 = zzero<T>(), dprev = zzero<T>();
+        double aprev = 0.0, gprev = 0.0;
+        if (live) {
+            rD0 = col[zpos(s0)];
+            if (s0 == 0 && periodic && pin) rD0 = zmul(0.5, zadd(rD0, col[zpos(nz - 1)]));
+            for (int i = 1; i < M; ++i) {
                 const int gk = s0 + i;
+                const T D = col[zpos(gk)];
                 double A = 1.0, B = lam, C = 1.0;
-                if (gk == 0) {
-                    A = A0;
-                    B = B0;
-                    C = C0;
-                } else if (gk == nz - 1) {
+                if (gk == nz - 1) {
                     A = AN;
                     B = BN;
                     C = CN;
                 }
-                T D = col[zpos(gk)];
-                if (gk == 0 && periodic && pin) D = zmul(0.5, zadd(D, col[zpos(nz - 1)]));
-                if (i == 0) {
-                    rA0 = A;
-                    rB0 = B;
-                    rC0 = C;
-                    rD0 = D;
-                    al[0] = 0.0;
-                    ga[0] = 0.0;
+                double al, ga;
+                T dn;
+                if (i == 1) {
+                    const double inv = 1.0 / B;
+                    al = A * inv;
+                    ga = C * inv;
+                    dn = zmul(inv, D);
                 } else {
-                    T dn;
-                    if (i == 1) {
-                        const double inv = 1.0 / B;
-                        al[1] = A * inv;
-                        ga[1] = C * inv;
-                        dn = zmul(inv, D);
-                    } else {
-                        const double p = 1.0 / (B - A * ga[i - 1]);
-                        al[i] = -A * al[i - 1] * p;
-                        ga[i] = C * p;
-                        dn = zmul(p, zsub(D, zmul(A, dprev)));
-                    }
-                    col[zpos(gk)] = dn;
-                    dprev = dn;
-                    if (i == M - 1) {
-                        e1a = al[i];
-                        e1c = ga[i];
-                        e1d = dn;
-                    }
+                    const double p = 1.0 / (B - A * gprev);
+                    al = -A * aprev * p;
+                    ga = C * p;
+                    dn = zmul(p, zsub(D, zmul(A, dprev)));
                 }
+                col[zpos(gk)] = dn;
+                if (lane == 0) tab[i] = make_double2(ga, al);
+                aprev = al;
+                gprev = ga;
+                dprev = dn;
             }
         }
-        // backward sweep: row 1 in terms of the block's first and last unknowns
+        // (alpha, gamma, delta) of the block's last row: the reduced row E1
+        const double e1a = aprev, e1c = gprev;
+        const T e1d = dprev;
+        __syncwarp(full);
+
+        // ---- backward sweep: row 1 in terms of x_0 and x_{M-1} ------------------------
         double br = 0, cr = 0;
         T dr = zzero<T>();
-#pragma unroll
-        for (int i = MMAX - 1; i >= 1; --i) {
-            if (i <= M - 2) {
-                const T di = col[zpos(s0 + i)];
-                if (i == M - 2) {
-                    br = al[i];
-                    cr = ga[i];
-                    dr = di;
-                } else {
-                    dr = zsub(di, zmul(ga[i], dr));
-                    br = al[i] - ga[i] * br;
-                    cr = -ga[i] * cr;
-                }
+        if (live && M >= 3) {
+            const double2 t2 = tab[M - 2];
+            br = t2.y;
+            cr = t2.x;
+            dr = col[zpos(s0 + M - 2)];
+            for (int i = M - 3; i >= 1; --i) {
+                const double2 ti = tab[i];
+                dr = zsub(col[zpos(s0 + i)], zmul(ti.x, dr));
+                br = ti.y - ti.x * br;
+                cr = -ti.x * cr;
             }
         }
         double e0a, e0c;
@@ -206,23 +228,21 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             e0d = zmul(q, zsub(rD0, zmul(rC0, dr)));
         }
 
-        // ---- reduced system: rows 2L (first) and 2L+1 (last), unit diagonal ---
-        if (active) {
-            ra[2 * lane] = e0a;
-            rc[2 * lane] = e0c;
-            rd[2 * lane] = e0d;
-            ru[2 * lane] = 0.0;
-            ra[2 * lane + 1] = e1a;
-            rc[2 * lane + 1] = e1c;
-            rd[2 * lane + 1] = e1d;
-            ru[2 * lane + 1] = 0.0;
-        }
-        __syncwarp();
+        // ---- reduced system: rows 2L (first) and 2L+1 (last), unit diagonal ---------
+        ra[2 * lane] = e0a;
+        rc[2 * lane] = e0c;
+        rd[2 * lane] = e0d;
+        ru[2 * lane] = 0.0;
+        ra[2 * lane + 1] = e1a;
+        rc[2 * lane + 1] = e1c;
+        rd[2 * lane + 1] = e1d;
+        ru[2 * lane + 1] = 0.0;
+        __syncwarp(full);
         double beta = 0.0;
         const double gam = -1.0;
         if (periodic && lane == 0) {
-            // Sherman-Morrison on the reduced cyclic system: corners move into
-            // u v^T with u = (gam, 0, .., alpha), v = (1, 0, .., beta / gam)
+            // Sherman-Morrison on the reduced cyclic system: the corners move
+            // into u v^T with u = (gam, 0, .., alpha), v = (1, 0, .., beta / gam)
             beta = ra[0];
             const double alpha = rc[m - 1];
             ra[0] = 0.0;
@@ -236,125 +256,138 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             rd[m - 1] = zmul(1.0 / bl, rd[m - 1]);
             ru[m - 1] = alpha / bl;
         }
-        __syncwarp();
+        __syncwarp(full);
         for (int st = 1; st < m; st <<= 1) {
             double na[2], nc[2], nu[2];
             T nd[2];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int r = 2 * lane + h;
-                if (active) {
-                    const double k1 = ra[r], k2 = rc[r];
-                    double a1 = 0, c1 = 0, u1 = 0, a2 = 0, c2 = 0, u2 = 0;
-                    T d1 = zzero<T>(), d2 = zzero<T>();
-                    if (r - st >= 0) {
-                        a1 = ra[r - st];
-                        c1 = rc[r - st];
-                        u1 = ru[r - st];
-                        d1 = rd[r - st];
-                    }
-                    if (r + st < m) {
-                        a2 = ra[r + st];
-                        c2 = rc[r + st];
-                        u2 = ru[r + st];
-                        d2 = rd[r + st];
-                    }
-                    const double inv = 1.0 / (1.0 - k1 * c1 - k2 * a2);
-                    na[h] = -k1 * a1 * inv;
-                    nc[h] = -k2 * c2 * inv;
-                    nu[h] = (ru[r] - k1 * u1 - k2 * u2) * inv;
-                    nd[h] = zmul(inv, zsub(zsub(rd[r], zmul(k1, d1)), zmul(k2, d2)));
+                const double k1 = ra[r], k2 = rc[r];
+                double a1 = 0, c1 = 0, u1 = 0, a2 = 0, c2 = 0, u2 = 0;
+                T d1 = zzero<T>(), d2 = zzero<T>();
+                if (r - st >= 0) {
+                    a1 = ra[r - st];
+                    c1 = rc[r - st];
+                    u1 = ru[r - st];
+                    d1 = rd[r - st];
                 }
+                if (r + st < m) {
+                    a2 = ra[r + st];
+                    c2 = rc[r + st];
+                    u2 = ru[r + st];
+                    d2 = rd[r + st];
+                }
+                const double inv = 1.0 / (1.0 - k1 * c1 - k2 * a2);
+                na[h] = -k1 * a1 * inv;
+                nc[h] = -k2 * c2 * inv;
+                nu[h] = (ru[r] - k1 * u1 - k2 * u2) * inv;
+                nd[h] = zmul(inv, zsub(zsub(rd[r], zmul(k1, d1)), zmul(k2, d2)));
             }
-            __syncwarp();
-            if (active) {
+            __syncwarp(full);
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int r = 2 * lane + h;
-                    ra[r] = na[h];
-                    rc[r] = nc[h];
-                    ru[r] = nu[h];
-                    rd[r] = nd[h];
-                }
+            for (int h = 0; h < 2; ++h) {
+                const int r = 2 * lane + h;
+                ra[r] = na[h];
+                rc[r] = nc[h];
+                ru[r] = nu[h];
+                rd[r] = nd[h];
             }
-            __syncwarp();
+            __syncwarp(full);
         }
-        T xf = zzero<T>(), xl = zzero<T>();
+        T xf, xl;
         if (periodic) {
             // fact = (y_0 + (beta/gam) y_{m-1}) / (1 + z_0 + (beta/gam) z_{m-1})
-            const double b = __shfl_sync(0xffffffffu, beta, 0);
+            const double b = __shfl_sync(full, beta, threadIdx.x & ~(P - 1) & 31);
             const double bg = b / gam;
-            const T y0 = rd[0], yl = rd[m - 1];
             const double den = 1.0 + ru[0] + bg * ru[m - 1];
-            const T fact = zmul(1.0 / den, zadd(y0, zmul(bg, yl)));
-            if (active) {
-                xf = zsub(rd[2 * lane], zmul(ru[2 * lane], fact));
-                xl = zsub(rd[2 * lane + 1], zmul(ru[2 * lane + 1], fact));
-            }
-        } else if (active) {
+            const T fact = zmul(1.0 / den, zadd(rd[0], zmul(bg, rd[m - 1])));
+            xf = zsub(rd[2 * lane], zmul(ru[2 * lane], fact));
+            xl = zsub(rd[2 * lane + 1], zmul(ru[2 * lane + 1], fact));
+        } else {
             xf = rd[2 * lane];
             xl = rd[2 * lane + 1];
         }
-        __syncwarp();
+        __syncwarp(full);
 
-        // ---- recover the block's rows -----------------------------------------
-        if (active) {
+        // ---- recover the block's rows ---------------------------------------------------
+        if (live) {
             T xn = xl;
             col[zpos(s0 + M - 1)] = xl;
-#pragma unroll
-            for (int i = MMAX - 1; i >= 1; --i) {
-                if (i <= M - 2) {
-                    xn = zsub(zsub(col[zpos(s0 + i)], zmul(al[i], xf)), zmul(ga[i], xn));
-                    col[zpos(s0 + i)] = xn;
-                }
+            for (int i = M - 2; i >= 1; --i) {
+                const double2 ti = tab[i];
+                xn = zsub(zsub(col[zpos(s0 + i)], zmul(ti.y, xf)), zmul(ti.x, xn));
+                col[zpos(s0 + i)] = xn;
             }
             col[zpos(s0)] = xf;
         }
-        __syncwarp();
+        __syncwarp(full);
     }
     __syncthreads();
 
     for (int idx = threadIdx.x; idx < ts * nz; idx += blockDim.x) {
         const int k = idx / ts;
         const int s = idx - k * ts;
-        g[k * plane + col0 + s] = tile[s * pitch + zpos(k)];
+        g[k * plane + col0 + s] = tile[s * Lz.pitch + zpos(k)];
     }
-}
-
-template <bool CPLX>
-cudaError_t launch_m(const PPZArgs& a, size_t smem, cudaStream_t st)
-{
-    const int P = a.nz / 2 < 32 ? a.nz / 2 : 32;
-    const int mneed = (a.nz + P - 1) / P;
-    dim3 grid(a.ny * a.tiles_x), block(PP_Z_THREADS);
-#define PP_ZL(MM)                                                                                           \
-    do {                                                                                                    \
-        auto kfn = zsolve_kernel<CPLX, MM>;                                                                 \
-        cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        if (e != cudaSuccess) return e;                                                                     \
-        kfn<<<grid, block, smem, st>>>(a);                                                                  \
-        return cudaGetLastError();                                                                          \
-    } while (0)
-    if (mneed <= 4) PP_ZL(4);
-    if (mneed <= 8) PP_ZL(8);
-    if (mneed <= 16) PP_ZL(16);
-    if (mneed <= 32) PP_ZL(32);
-#undef PP_ZL
-    return cudaErrorInvalidValue;
 }
 
 }  // namespace
 
-size_t pp_zsolve_smem(int TS, int nz, bool cplx)
+int pp_zsolve_lanes(int nz, bool cplx)
 {
-    const size_t e = cplx ? 2 : 1;
-    return (size_t)TS * zpitch(nz) * e * sizeof(double) +
-           (size_t)(PP_Z_THREADS / 32) * RED_ROWS * (3 + e) * sizeof(double);
+    // about 32 rows per lane (16 for complex data, whose tile is twice as
+    // large, so that a CTA still keeps every group busy)
+    const int rows = cplx ? 16 : 32;
+    int P = 1;
+    while (P < 32 && 2 * P <= nz / rows) P *= 2;
+    while (P > 1 && P > nz / 2) P /= 2;
+    return P;
 }
 
-cudaError_t pp_launch_zsolve(const PPZArgs& a, bool cplx, cudaStream_t st)
+// launch shape: systems per CTA (one lane group each) and threads per CTA,
+// keeping the CTA within ~112 KB of shared memory so two fit on an SM
+void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads)
 {
-    if (a.nz < 3 || a.nz > PP_Z_MAX_NZ) return cudaErrorInvalidValue;
+    const int P = pp_zsolve_lanes(nz, cplx);
+    int ts = PP_Z_THREADS / P;
+    auto bytes = [&](int t) {
+        const int th = t * P < 32 ? 32 : t * P;
+        return zlayout(t, nz, P, cplx, th).bytes;
+    };
+    while (ts > 1 && bytes(ts) > 112 * 1024) ts >>= 1;
+    while (ts > 1 && ts > nx) ts >>= 1;
+    *TS = ts;
+    *threads = ts * P < 32 ? 32 : ts * P;
+}
+
+size_t pp_zsolve_smem(int TS, int nz, bool cplx)
+{
+    const int P = pp_zsolve_lanes(nz, cplx);
+    const int th = TS * P < 32 ? 32 : TS * P;
+    return zlayout(TS, nz, P, cplx, th).bytes;
+}
+
+cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
+{
+    if (a0.nz < 3 || a0.nz > PP_Z_MAX_NZ) return cudaErrorInvalidValue;
+    PPZArgs a = a0;
+    a.P = pp_zsolve_lanes(a.nz, cplx);
+    const int threads = a.TS * a.P < 32 ? 32 : a.TS * a.P;
+    if (threads > PP_Z_THREADS) return cudaErrorInvalidValue;
     const size_t smem = pp_zsolve_smem(a.TS, a.nz, cplx);
-    return cplx ? launch_m<true>(a, smem, st) : launch_m<false>(a, smem, st);
+    dim3 grid(a.ny * a.tiles_x), block(threads);
+    cudaError_t e;
+    if (cplx) {
+        auto kfn = zsolve_kernel<true>;
+        if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+            return e;
+        kfn<<<grid, block, smem, st>>>(a);
+    } else {
+        auto kfn = zsolve_kernel<false>;
+        if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+            return e;
+        kfn<<<grid, block, smem, st>>>(a);
+    }
+    return cudaGetLastError();
 }

@@ -56,11 +56,12 @@ def _valid(bcx, bcy):
 CASES = [(x, y, z) for x in FAMILIES for y in FAMILIES for z in ZBC if _valid(x, y)]
 
 
+@pytest.mark.parametrize("shape", [(24, 20, 18), (32, 16, 40)], ids=["generic_fft", "pow2_fft"])
 @pytest.mark.parametrize("bcx,bcy,bcz", CASES)
-def test_all_families_vs_oracle(bcx, bcy, bcz):
+def test_all_families_vs_oracle(bcx, bcy, bcz, shape):
     bc = bcx + bcy + bcz
     rng = np.random.default_rng(abs(hash(bc)) % 2**32)
-    nx, ny, nz = 24, 20, 18
+    nx, ny, nz = shape
     f = rng.uniform(-1, 1, (nz, ny, nx))
     if bcx == "PP" or bcy == "PP":
         f = f + 1j * rng.uniform(-1, 1, (nz, ny, nx))
@@ -72,7 +73,7 @@ def test_all_families_vs_oracle(bcx, bcy, bcz):
 
 
 @pytest.mark.parametrize("shape", [(30, 48, 20), (96, 10, 7), (12, 160, 33), (64, 64, 3), (2, 6, 4), (50, 45, 4),
-                                   (128, 96, 100)])
+                                   (128, 96, 100), (16, 2048, 5), (1024, 16, 9), (256, 128, 64)])
 @pytest.mark.parametrize("bc", ["NNDDNN", "PPPPDD", "DDNNPP", "DNPPDN", "NDDDND"])
 def test_sizes_vs_oracle(shape, bc):
     nx, ny, nz = shape
