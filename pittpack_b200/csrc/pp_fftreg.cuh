@@ -72,6 +72,12 @@ constexpr int rp_ns(int n, int pass)
     for (int i = 0; i < pass; ++i) ns *= rp_radix(n, i);
     return ns;
 }
+constexpr int rp_log2(int n)
+{
+    int l = 0;
+    while ((1 << l) < n) ++l;
+    return l;
+}
 // padded slot of point i, and an odd line pitch
 PP_HD constexpr int rp_pad(int i) { return i + (i >> 3); }
 PP_HD constexpr int rp_pitch(int n) { return ((rp_pad(n - 1) + 1) | 1); }

@@ -34,6 +34,17 @@ PP_D double lift2(const PPLift& L, int i, int j, int k, int nx, int ny, int nz)
     return s;
 }
 
+PP_D void cp_async8(void* smem, const void* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+PP_D void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
 template <typename T>
 struct Vec2;
 template <>
@@ -98,56 +109,67 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     const C* cs = reinterpret_cast<const C*>(a.cs2);
 
     // ---- 1. load the raw tile ---------------------------------------------------------
-    // lines beyond nl (last tile of a plane) are zero-filled so every FFT line is defined
+    // Every element is copied asynchronously (cp.async, no register staging)
+    // straight to its slot in the FFT buffer: the family's reorder / reversal
+    // is the slot; signs and the RHS scaling are applied later.  Lines beyond
+    // nl (last tile of a plane) are zero-filled.
+    const int ldl = __ffs(DL) - 1;
+    constexpr int LN = rp_log2(N);
     const int total = DL * N;
+    // slot (in Real units) of element e of data line l
+    auto slot = [&](int l, int e) -> int {
+        if (fftk) return 2 * (l * P1 + rp_pad(e));
+        if (quarter) return l * 2 * P4 + ((kind == PP_KIND_DST4) ? (N - 1 - e) : e);
+        int pos;
+        if (!INVERSE) pos = mk_pos(kind == PP_KIND_DCT2 ? e : N - 1 - e, N);
+        else pos = (kind == PP_KIND_DCT2) ? e : N - 1 - e;
+        return 2 * ((l >> 1) * P1 + rp_pad(pos)) + (l & 1);
+    };
     for (int idx = tid; idx < total; idx += NT) {
         int l, e;
         if (STRIDED) {
-            l = idx % DL;
-            e = idx / DL;
+            l = idx & (DL - 1);
+            e = idx >> ldl;
         } else {
-            l = idx / N;
-            e = idx - l * N;
+            l = idx >> LN;
+            e = idx & (N - 1);
         }
-        Real re = 0, im = 0;
+        Real* d = sr + slot(l, e);
         if (l < nl) {
             const long off = base + (long)l * a.line_stride + (long)e * a.elem_stride;
-            gload<TI, Real>(a.src, off, a.in_cplx, re, im);
-            if (a.rhs_scale) {
-                re = re * (Real)a.dz * (Real)a.dz;
-                im = im * (Real)a.dz * (Real)a.dz;
-                if (a.lift.any) re = re - (Real)lift2(a.lift, e, l0 + l, plane, a.nx, a.ny, a.nz);
-            }
-        }
-        if (fftk) {
-            sb[l * P1 + rp_pad(e)] = mkc<C>(re, im);
-        } else if (quarter) {
-            const int pos = (kind == PP_KIND_DST4) ? (N - 1 - e) : e;
-            sr[l * 2 * P4 + pos] = re;
-        } else {
-            // packed pair: line l -> complex line l/2, component l%2
-            int pos;
-            Real v = re;
-            if (!INVERSE) {
-                if (kind == PP_KIND_DCT2) {
-                    pos = mk_pos(e, N);
-                } else {  // DST-II: x'[j] = (-1)^j x[N-1-j], then the reorder
-                    const int j = N - 1 - e;
-                    if (j & 1) v = -v;
-                    pos = mk_pos(j, N);
-                }
+            if (sizeof(TI) == sizeof(Real) && fftk && a.in_cplx) {
+                cp_async16(d, reinterpret_cast<const TI*>(a.src) + 2 * off);
+            } else if (sizeof(TI) == sizeof(Real)) {
+                cp_async8(d, reinterpret_cast<const TI*>(a.src) + (a.in_cplx ? 2 * off : off));
+                if (fftk) d[1] = (Real)0;
             } else {
-                if (kind == PP_KIND_DCT2) {
-                    pos = e;
-                } else {  // DST-III: swap first
-                    pos = N - 1 - e;
-                    if (pos & 1) v = -v;
-                }
+                // precision change on the way in: plain loads
+                Real re, im;
+                gload<TI, Real>(a.src, off, a.in_cplx, re, im);
+                d[0] = re;
+                if (fftk) d[1] = im;
             }
-            sr[2 * ((l >> 1) * P1 + rp_pad(pos)) + (l & 1)] = v;
+        } else {
+            d[0] = (Real)0;
+            if (fftk) d[1] = (Real)0;
         }
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
+    if (a.rhs_scale) {
+        // forward x pass: f dz dz minus the Dirichlet lift (assignRhs, modifyRhsDirichlet)
+        for (int idx = tid; idx < nl * N; idx += NT) {
+            const int l = idx >> LN;
+            const int e = idx & (N - 1);
+            Real* d = sr + slot(l, e);
+            Real re = d[0] * (Real)a.dz * (Real)a.dz;
+            if (a.lift.any) re = re - (Real)lift2(a.lift, e, l0 + l, plane, a.nx, a.ny, a.nz);
+            d[0] = re;
+            if (fftk) d[1] = d[1] * (Real)a.dz * (Real)a.dz;
+        }
+        __syncthreads();
+    }
 
     // ---- 2. pre-processing into the pass-0 registers and 3. FFT --------------------
     C v[8];
@@ -161,8 +183,12 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
 #pragma unroll
             for (int q = 0; q < R0; ++q) {
                 const int m = rp_in_index<N>(t, g, q);
-                if (fftk || !INVERSE) {
+                if (fftk) {
                     v[g * R0 + q] = line[rp_pad(m)];
+                } else if (!INVERSE) {
+                    // DST-II: x'[j] = (-1)^j x[N-1-j]; odd j land in the upper half
+                    const C z = line[rp_pad(m)];
+                    v[g * R0 + q] = (kind == PP_KIND_DST2 && m >= N / 2) ? mkc<C>(-z.x, -z.y) : z;
                 } else {
                     // DCT-III pre-processing of both packed spectra; Z = V1 + i V2
                     const C Xm = line[rp_pad(m)];
@@ -182,7 +208,10 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                             V2 = mkc<C>((Real)0.5 * (w.x * Xn.y + w.y * Xm.y), -((Real)0.5 * (w.y * Xn.y - w.x * Xm.y)));
                         }
                     }
-                    v[g * R0 + q] = mkc<C>(V1.x - V2.y, V1.y + V2.x);
+                    C Z = mkc<C>(V1.x - V2.y, V1.y + V2.x);
+                    // DST-III: the swapped input carries (-1)^m at slots m and N-m
+                    if (kind == PP_KIND_DST2 && (m & 1)) Z = mkc<C>(-Z.x, -Z.y);
+                    v[g * R0 + q] = Z;
                 }
             }
         if (INVERSE && !fftk) rp_fft<+1, N>(v, line, t, tw);
@@ -229,11 +258,11 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     for (int idx = tid; idx < total; idx += NT) {
         int l, e;
         if (STRIDED) {
-            l = idx % DL;
-            e = idx / DL;
+            l = idx & (DL - 1);
+            e = idx >> ldl;
         } else {
-            l = idx / N;
-            e = idx - l * N;
+            l = idx >> LN;
+            e = idx & (N - 1);
         }
         if (l >= nl) continue;
         Real re, im = 0;

@@ -50,6 +50,20 @@ PP_D double zzero<double>() { return 0.0; }
 template <>
 PP_D double2 zzero<double2>() { return make_double2(0.0, 0.0); }
 
+// asynchronous global -> shared copies (LDGSTS): no register staging, every
+// copy of a tile in flight at once
+PP_D void cp_async8(void* smem, const void* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+PP_D void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+PP_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // skewed position of row k inside a system's column of the tile
 PP_HD int zpos(int k) { return k + (k >> 4); }
 PP_HD int zpitch(int nz) { return (zpos(nz - 1) + 1) | 1; }
@@ -74,7 +88,7 @@ PP_HD ZLayout zlayout(int TS, int nz, int P, bool cplx, int nthreads)
     L.tile_off = 0;
     L.tab_off = (size_t)TS * L.pitch * e;
     L.tab_off = (L.tab_off + 15) & ~(size_t)15;
-    L.red_off = L.tab_off + (size_t)L.groups * L.mmax * 16;
+    L.red_off = L.tab_off + (size_t)TS * L.mmax * 16;
     // per group: 2P rows of a, c, u (doubles) and d (element)
     L.bytes = L.red_off + (size_t)L.groups * 2 * P * (24 + e);
     return L;
@@ -92,7 +106,6 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
 
     const int group = threadIdx.x / P;
     const int lane = threadIdx.x - group * P;
-    double2* tab = reinterpret_cast<double2*>(zsm_raw + Lz.tab_off) + (size_t)group * Lz.mmax;  // (p_i, alpha_i)
     const int m = 2 * P;
     unsigned char* redb = zsm_raw + Lz.red_off + (size_t)group * m * (24 + sizeof(T));
     double* ra = reinterpret_cast<double*>(redb);
@@ -107,11 +120,49 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     const long plane = (long)nx * ny;
     const long col0 = (long)ky * nx + kx0;
 
-    for (int idx = threadIdx.x; idx < ts * nz; idx += blockDim.x) {
-        const int k = idx / ts;
-        const int s = idx - k * ts;
-        tile[s * Lz.pitch + zpos(k)] = g[k * plane + col0 + s];
+    // ---- load the tile asynchronously (thread -> (system, row) without division:
+    //      TS is a power of two) and build the pivot tables while it lands ------------
+    const int lts = __ffs(a.TS) - 1;
+    {
+        const int s = threadIdx.x & (a.TS - 1);
+        const int kstep = blockDim.x >> lts;
+        if (s < ts)
+            for (int k = threadIdx.x >> lts; k < nz; k += kstep)
+                if (sizeof(T) == 16) cp_async16(&tile[s * Lz.pitch + zpos(k)], &g[k * plane + col0 + s]);
+                else cp_async8(&tile[s * Lz.pitch + zpos(k)], &g[k * plane + col0 + s]);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
+    // interior pivots of a block, depending only on lambda: with b_0 = 1,
+    // b_1 = lambda, b_i = lambda b_{i-1} - b_{i-2} (Chebyshev U_i(lambda/2)),
+    //   gamma_i = b_{i-1} / b_i,  alpha_i = (-1)^{i-1} / b_i,
+    // the same numbers as the Thomas recurrence gamma_i = 1 / (lambda - gamma_{i-1}).
+    // One thread per system; the divisions are independent.  For |lambda| > 1e3
+    // the b_i could overflow, so the division recurrence is used instead.
+    for (int s = threadIdx.x; s < ts; s += blockDim.x) {
+        const double lam = (-2.0 + a.ax[kx0 + s] * a.Cx) + a.ay[ky] * a.Cy;
+        double2* tb = reinterpret_cast<double2*>(zsm_raw + Lz.tab_off) + (size_t)s * Lz.mmax;
+        const int mm = Lz.mmax;
+        if (fabs(lam) <= 1.0e3) {
+            double bm = 1.0, bc = lam, sg = 1.0;
+            for (int i = 1; i < mm; ++i) {
+                tb[i] = make_double2(bm / bc, sg / bc);
+                const double bn = lam * bc - bm;
+                bm = bc;
+                bc = bn;
+                sg = -sg;
+            }
+        } else {
+            double gp = 0.0, ap = 0.0;
+            for (int i = 1; i < mm; ++i) {
+                const double p = (i == 1) ? 1.0 / lam : 1.0 / (lam - gp);
+                const double al = (i == 1) ? p : -ap * p;
+                tb[i] = make_double2(p, al);
+                gp = p;
+                ap = al;
+            }
+        }
+    }
+    cp_async_wait_all();
     __syncthreads();
 
     const int bsz = nz / P;
@@ -133,6 +184,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         const bool zero = fabs(lam + 2.) < 1.e-10;
         const bool pin = zero && (periodic || a.pin_always || !has_d);
         T* col = tile + (live ? s : 0) * Lz.pitch;
+        const double2* tab = reinterpret_cast<const double2*>(zsm_raw + Lz.tab_off) + (size_t)(live ? s : 0) * Lz.mmax;
 
         double A0, B0, C0, AN, BN, CN;
         if (periodic) {
@@ -168,27 +220,25 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             for (int i = 1; i < M; ++i) {
                 const int gk = s0 + i;
                 const T D = col[zpos(gk)];
-                double A = 1.0, B = lam, C = 1.0;
-                if (gk == nz - 1) {
-                    A = AN;
-                    B = BN;
-                    C = CN;
-                }
                 double al, ga;
                 T dn;
-                if (i == 1) {
-                    const double inv = 1.0 / B;
-                    al = A * inv;
-                    ga = C * inv;
+                if (gk != nz - 1) {
+                    const double2 t = tab[i];
+                    ga = t.x;
+                    al = t.y;
+                    dn = (i == 1) ? zmul(ga, D) : zmul(ga, zsub(D, dprev));
+                } else if (i == 1) {
+                    const double inv = 1.0 / BN;
+                    al = AN * inv;
+                    ga = CN * inv;
                     dn = zmul(inv, D);
                 } else {
-                    const double p = 1.0 / (B - A * gprev);
-                    al = -A * aprev * p;
-                    ga = C * p;
-                    dn = zmul(p, zsub(D, zmul(A, dprev)));
+                    const double p = 1.0 / (BN - AN * gprev);
+                    al = -AN * aprev * p;
+                    ga = CN * p;
+                    dn = zmul(p, zsub(D, zmul(AN, dprev)));
                 }
                 col[zpos(gk)] = dn;
-                if (lane == 0) tab[i] = make_double2(ga, al);
                 aprev = al;
                 gprev = ga;
                 dprev = dn;
@@ -325,10 +375,11 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     }
     __syncthreads();
 
-    for (int idx = threadIdx.x; idx < ts * nz; idx += blockDim.x) {
-        const int k = idx / ts;
-        const int s = idx - k * ts;
-        g[k * plane + col0 + s] = tile[s * Lz.pitch + zpos(k)];
+    {
+        const int s = threadIdx.x & (a.TS - 1);
+        const int kstep = blockDim.x >> lts;
+        if (s < ts)
+            for (int k = threadIdx.x >> lts; k < nz; k += kstep) g[k * plane + col0 + s] = tile[s * Lz.pitch + zpos(k)];
     }
 }
 
