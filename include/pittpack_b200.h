@@ -51,9 +51,12 @@ typedef struct pp_solver_s* pp_handle;
 /* runtime options; the reference keeps these as compile-time switches in
  * src/include/params.h (SOLUTIONMETHOD, NITER, ...) */
 typedef struct {
-    int precision;        /* PP_PRECISION_FP64 (default) */
-    int max_sweeps;       /* refinement sweeps for PP_PRECISION_MIXED */
-    double tolerance;     /* relative residual target for PP_PRECISION_MIXED */
+    int precision;        /* PP_PRECISION_FP64 (default) or PP_PRECISION_MIXED: FP32
+                             transforms + FP64 iterative refinement of the true
+                             7-point system (exact zero mode); real RHS and
+                             power-of-two nx, ny */
+    int max_sweeps;       /* refinement sweeps after the first FP32 solve (0..16) */
+    double tolerance;     /* target the caller checks; sweeps are a fixed count (no host sync) */
     int compat_zero_mode; /* 1 (default): reference zero-mode row replacement, src/triDiag.cpp:1753-1776 */
     int dirichlet_lift;   /* 1 (default): reference modifyRhsDirichlet, src/pencilDcmp.cpp:4623-4835 */
 } pp_options;
@@ -92,15 +95,17 @@ int pp_assign_rhs_device(pp_handle h, const double* d_rhs, int is_complex);
 int pp_solve(pp_handle h);
 /* profiling hook, no counterpart in the reference (which times the whole
  * solve with MPI_Wtime, src/pencilDcmp.cpp:5900-6333): one solve with CUDA
- * events between its kernels; kernel_ms[0..4] = forward x, forward y, z solve,
- * inverse y, inverse x (milliseconds).  Synchronises the handle's stream. */
-#define PP_SOLVE_KERNELS 5
+ * events around its stages; kernel_ms[0..5] = forward x, forward y, z solve,
+ * inverse y, inverse x, residual + zero mode (refined solve only), in
+ * milliseconds summed over the sweeps.  Synchronises the handle's stream. */
+#define PP_SOLVE_STAGES 6
 int pp_profile_solve(pp_handle h, double* kernel_ms, int n);
-/* live per-kernel timing, no counterpart in the reference: between
+/* live per-stage timing, no counterpart in the reference: between
  * pp_timing_begin and pp_timing_end the first max_solves calls of pp_solve
- * record CUDA events between their kernels on the handle's stream (no extra
+ * record CUDA events around their stages on the handle's stream (no extra
  * synchronisation); pp_timing_end waits for the last one and returns the
- * summed milliseconds per kernel and the number of solves recorded. */
+ * summed milliseconds per stage (PP_SOLVE_STAGES slots, as pp_profile_solve)
+ * and the number of solves recorded. */
 int pp_timing_begin(pp_handle h, int max_solves);
 int pp_timing_end(pp_handle h, double* kernel_ms_total, int n, int* solves);
 /* the solution P (2*nx*ny*nz doubles, chunkedArray layout) to host memory;

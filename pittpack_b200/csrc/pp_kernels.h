@@ -46,6 +46,13 @@ struct PPLinePassArgs {
     const void* tw;    // FFT twiddles (double2 or float2), length n or n/2
     const void* cs2;   // family twiddles in the kernel's precision
     int in_cplx, out_cplx;
+    // refinement epilogue of the inverse x pass (acc != null): the real part v
+    // of each output becomes u = acc + out_scale v + zplane[plane] in FP64;
+    // written to acc, or (dst != null) as the final complex-interleaved P
+    double* acc;
+    const double* zplane;
+    double zscale;      // zplane[plane] is multiplied by this
+    int acc_read;       // 0: the previous u is zero (first sweep), acc is not read
 };
 
 size_t pp_line_pass_smem(int L, int nfft);
@@ -72,6 +79,8 @@ struct PPZArgs {
     int zlo, zhi;       // PPZBc of the two z ends
     int pin_always;     // 1: zero-mode row replacement whatever the z ends (reference)
     int P;              // lanes per system (set by the launcher)
+    int data_fp32;      // spectrum stored as float / float2 (solved in FP64)
+    int skip_zero;      // write zeros for the kx = ky = 0 column
 };
 
 // lanes that share one z system (a power of two <= 32)
@@ -80,4 +89,23 @@ int pp_zsolve_lanes(int nz, bool cplx);
 void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads);
 
 size_t pp_zsolve_smem(int TS, int nz, bool cplx);
+
+// FP64 residual r = f dz^2 - lift - A u of the refined solve (pp_mixed.cu)
+struct PPResidArgs {
+    const double* f;   // real RHS, unscaled
+    const double* u;   // current solution (real), or null for u = 0
+    float* r;          // FP32 residual out
+    double* psum;      // per-plane sums of r times psum_scale (zero mode), or null
+    double psum_scale;
+    int nx, ny, nz;
+    double dz, Cx, Cy;
+    int bc[6];         // face codes: 0 Dirichlet, 1 Neumann, 2 periodic
+    PPLift lift;
+    double* usum;      // FP64 sum of u over the grid, or null
+};
+cudaError_t pp_launch_resid(const PPResidArgs& a, cudaStream_t st);
+// Singular problems: keep the null-space constant of the refined solution at
+// the value implied by the pinned FP64 zero-mode solve of b (see pp_mixed.cu).
+cudaError_t pp_launch_zero_mode_anchor(double* zcol, int nz, const double* usum, double* mstar, double zscale,
+                                       double npts, int first, cudaStream_t st);
 cudaError_t pp_launch_zsolve(const PPZArgs& a, bool cplx, cudaStream_t st);

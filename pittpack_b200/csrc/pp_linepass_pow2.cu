@@ -34,15 +34,14 @@ PP_D double lift2(const PPLift& L, int i, int j, int k, int nx, int ny, int nz)
     return s;
 }
 
-PP_D void cp_async8(void* smem, const void* gmem)
+// asynchronous global -> shared copy of BYTES (4, 8 or 16)
+template <int BYTES>
+PP_D void cp_async(void* smem, const void* gmem)
 {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-PP_D void cp_async16(void* smem, const void* gmem)
-{
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+    if (BYTES == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+    if (BYTES == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+    if (BYTES == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 
 template <typename T>
@@ -138,9 +137,9 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
         if (l < nl) {
             const long off = base + (long)l * a.line_stride + (long)e * a.elem_stride;
             if (sizeof(TI) == sizeof(Real) && fftk && a.in_cplx) {
-                cp_async16(d, reinterpret_cast<const TI*>(a.src) + 2 * off);
+                cp_async<2 * sizeof(TI)>(d, reinterpret_cast<const TI*>(a.src) + 2 * off);
             } else if (sizeof(TI) == sizeof(Real)) {
-                cp_async8(d, reinterpret_cast<const TI*>(a.src) + (a.in_cplx ? 2 * off : off));
+                cp_async<sizeof(TI)>(d, reinterpret_cast<const TI*>(a.src) + (a.in_cplx ? 2 * off : off));
                 if (fftk) d[1] = (Real)0;
             } else {
                 // precision change on the way in: plain loads
@@ -305,11 +304,19 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                 re = sg * (comp == 0 ? z.x : z.y);
             }
         }
+        const long off = base + (long)l * a.line_stride + (long)e * a.elem_stride;
+        if (a.acc) {
+            // u = u_prev + scale * correction + zero-mode constant, in FP64
+            const double u = (a.acc_read ? a.acc[off] : 0.0) + a.out_scale * (double)re +
+                             (a.zplane ? a.zscale * a.zplane[plane] : 0.0);
+            if (a.dst) reinterpret_cast<double2*>(a.dst)[off] = make_double2(u, 0.0);
+            else a.acc[off] = u;
+            continue;
+        }
         if (osc != (Real)1) {
             re = osc * re;
             im = osc * im;
         }
-        const long off = base + (long)l * a.line_stride + (long)e * a.elem_stride;
         gstore<TO, Real>(a.dst, off, a.out_cplx, re, im);
     }
 }
@@ -380,3 +387,5 @@ cudaError_t pp_launch_line_pass_pow2(const PPLinePassArgs& a, bool inverse, bool
 
 template cudaError_t pp_launch_line_pass_pow2<double, double, double>(const PPLinePassArgs&, bool, bool,
                                                                       cudaStream_t);
+// the FP32 passes of the refined mixed-precision solve
+template cudaError_t pp_launch_line_pass_pow2<float, float, float>(const PPLinePassArgs&, bool, bool, cudaStream_t);

@@ -70,6 +70,8 @@ struct DirTables {
     DevBuf tw;   // FFT twiddles of length fft.n
     DevBuf cs;   // family pre/post twiddles
     DevBuf eig;  // -2 + 2 cos((k + num) f / (n + den)), k < n
+    DevBuf twf;  // FP32 copies for the refined mixed-precision solve
+    DevBuf csf;
 };
 
 }  // namespace
@@ -84,13 +86,22 @@ struct pp_solver_s {
     cudaStream_t stream = 0;
     DirTables tx, ty;
     DevBuf rhs, bufA, bufB, out;
+    DevBuf psum;   // refined solve: per-plane sums / zero-mode column (nz doubles)
+    DevBuf zero1;  // one double 0.0 (eigen table of the zero-mode system)
+    int last_sweeps = 0;
     DevBuf lift[6];
     PPLift liftv{};
     std::mutex mu;
     std::string last_error;
-    // live per-kernel timing (pp_timing_begin / pp_timing_end)
+    // live per-stage timing (pp_timing_begin / pp_timing_end): events from a
+    // pool, (stage, start event, end event) records, solves counted
+    struct TRec {
+        int slot, e0, e1;
+    };
     std::vector<cudaEvent_t> tev;
-    int tmax = 0, tcount = 0;
+    std::vector<TRec> trec;
+    int tnext = 0, tmax = 0, tcount = 0;
+    bool timing = false;
 };
 
 namespace {
@@ -157,6 +168,14 @@ int build_dir(pp_solver_s* h, DirTables& t, int n, int kind)
     if ((e = cudaMemcpy(t.eig.p, eig.data(), sizeof(double) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUDA_ERROR);
     t.fft.tw = t.tw.as<double2>();
+    // FP32 copies of the twiddles (rounded from the long-double / reference values)
+    std::vector<float2> twf(nf), csf(cs.size());
+    for (int m = 0; m < nf; ++m) twf[m] = make_float2((float)tw[m].x, (float)tw[m].y);
+    for (size_t m = 0; m < cs.size(); ++m) csf[m] = make_float2((float)cs[m].x, (float)cs[m].y);
+    if ((e = t.twf.alloc(sizeof(float2) * nf)) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+    if ((e = t.csf.alloc(sizeof(float2) * csf.size())) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+    cudaMemcpy(t.twf.p, twf.data(), sizeof(float2) * nf, cudaMemcpyHostToDevice);
+    cudaMemcpy(t.csf.p, csf.data(), sizeof(float2) * csf.size(), cudaMemcpyHostToDevice);
     return PP_SUCCESS;
 }
 
@@ -304,12 +323,39 @@ int pick_lines(int nfft)
     return L;
 }
 
+// timing stamps around one stage (no-ops unless timing is on)
+int stamp(pp_solver_s* h)
+{
+    if (!h->timing || h->tnext >= (int)h->tev.size()) return -1;
+    const int i = h->tnext++;
+    cudaEventRecord(h->tev[i], h->stream);
+    return i;
+}
+void stage_done(pp_solver_s* h, int slot, int i0)
+{
+    if (i0 < 0) return;
+    const int i1 = stamp(h);
+    if (i1 >= 0) h->trec.push_back({slot, i0, i1});
+}
+enum { SLOT_XF = 0, SLOT_YF = 1, SLOT_Z = 2, SLOT_YI = 3, SLOT_XI = 4, SLOT_RES = 5 };
+
 // one transform pass: the register-resident kernel for power-of-two lengths,
 // the generic shared-memory Stockham kernel otherwise
 cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool strided, bool in_cplx,
-                      bool out_cplx, cudaStream_t st)
+                      bool out_cplx, cudaStream_t st, bool fp32 = false)
 {
     const int lpc = pp_lp2_lpc(d.n);
+    if (fp32) {
+        if (lpc == 0) return cudaErrorInvalidValue;
+        a.tw = d.twf.p;
+        a.cs2 = d.csf.p;
+        a.in_cplx = in_cplx;
+        a.out_cplx = out_cplx;
+        const int dl = d.kind == PP_KIND_FFT ? lpc : 2 * lpc;
+        a.L = dl;
+        a.tiles_per_plane = (a.nlines + dl - 1) / dl;
+        return pp_launch_line_pass_pow2<float, float, float>(a, inverse, strided, st);
+    }
     if (lpc > 0) {
         a.tw = d.tw.p;
         a.cs2 = d.cs.p;
@@ -323,7 +369,7 @@ cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool s
     return pp_launch_line_pass(a, inverse, strided, in_cplx, out_cplx, st);
 }
 
-int launch_solve(pp_solver_s* h, cudaEvent_t* ev = nullptr)
+int launch_solve(pp_solver_s* h)
 {
     const int nx = h->nx, ny = h->ny, nz = h->nz;
     const int kx = h->tx.kind, ky = h->ty.kind;
@@ -332,7 +378,7 @@ int launch_solve(pp_solver_s* h, cudaEvent_t* ev = nullptr)
     const double dz = -(h->box[4] - h->box[5]) / (nz);
     const long plane = (long)nx * ny;
     cudaError_t e;
-    if (ev) cudaEventRecord(ev[0], h->stream);
+    int t0;
 
     PPLinePassArgs ax{};
     ax.n = nx;
@@ -369,16 +415,18 @@ int launch_solve(pp_solver_s* h, cudaEvent_t* ev = nullptr)
     a1.dst = h->bufA.as<double>();
     a1.rhs_scale = 1;
     a1.lift = h->liftv;
+    t0 = stamp(h);
     if ((e = line_pass(a1, h->tx, false, false, h->rhs_complex, x_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_X);
-    if (ev) cudaEventRecord(ev[1], h->stream);
+    stage_done(h, SLOT_XF, t0);
     // forward y: A -> B
     PPLinePassArgs a2 = ay;
     a2.src = h->bufA.as<double>();
     a2.dst = h->bufB.as<double>();
+    t0 = stamp(h);
     if ((e = line_pass(a2, h->ty, false, true, x_cplx, s_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_Y);
-    if (ev) cudaEventRecord(ev[2], h->stream);
+    stage_done(h, SLOT_YF, t0);
     // z solve in B
     PPZArgs z{};
     z.data = h->bufB.as<double>();
@@ -397,23 +445,190 @@ int launch_solve(pp_solver_s* h, cudaEvent_t* ev = nullptr)
     z.zlo = h->bc[4] == 'P' ? PP_Z_PERIODIC : (h->bc[4] == 'N' ? PP_Z_NEUMANN : PP_Z_DIRICHLET);
     z.zhi = h->bc[5] == 'P' ? PP_Z_PERIODIC : (h->bc[5] == 'N' ? PP_Z_NEUMANN : PP_Z_DIRICHLET);
     z.pin_always = h->opt.compat_zero_mode ? 1 : 0;
+    t0 = stamp(h);
     if ((e = pp_launch_zsolve(z, s_cplx, h->stream)) != cudaSuccess) return set_cuda_error(h, e, PP_THOMAS_FAIL);
-    if (ev) cudaEventRecord(ev[3], h->stream);
+    stage_done(h, SLOT_Z, t0);
     // inverse y: B -> A
     PPLinePassArgs a3 = ay;
     a3.src = h->bufB.as<double>();
     a3.dst = h->bufA.as<double>();
+    t0 = stamp(h);
     if ((e = line_pass(a3, h->ty, true, true, s_cplx, s_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_Y);
-    if (ev) cudaEventRecord(ev[4], h->stream);
+    stage_done(h, SLOT_YI, t0);
     // inverse x + rescale: A -> out (always complex-interleaved)
     PPLinePassArgs a4 = ax;
     a4.src = h->bufA.as<double>();
     a4.dst = h->out.as<double>();
     a4.out_scale = 1. / ((double)(nx * ny));
+    t0 = stamp(h);
     if ((e = line_pass(a4, h->tx, true, false, s_cplx, true, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_X);
-    if (ev) cudaEventRecord(ev[5], h->stream);
+    stage_done(h, SLOT_XI, t0);
+    return PP_SUCCESS;
+}
+
+bool has_zero_mode(int kx, int ky)
+{
+    return (kx == PP_KIND_DCT2 || kx == PP_KIND_FFT) && (ky == PP_KIND_DCT2 || ky == PP_KIND_FFT);
+}
+
+// Refined mixed-precision solve of the true discrete system A u = b:
+//   sweep 0:  r = b (FP64 -> FP32);            u = M32(r)
+//   sweep s:  r = b - A u (FP64 -> FP32);      u += M32(r)
+// M32 = FP32 transforms + FP64-arithmetic z solve on the FP32 spectrum with
+// the kx = ky = 0 column left out; that column (the only singular or nearly
+// singular one) is solved in FP64 from FP64 plane sums of r and added to u in
+// FP64.  The last sweep writes P.  Buffers: r (FP32) in the solution buffer,
+// FP32 spectra in the first halves of A and B, u (FP64) in the second half of B.
+int launch_mixed(pp_solver_s* h)
+{
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    const int kx = h->tx.kind, ky = h->ty.kind;
+    const bool x_cplx = kx == PP_KIND_FFT;
+    const bool s_cplx = ky == PP_KIND_FFT;
+    const bool zm = has_zero_mode(kx, ky);
+    const double dz = -(h->box[4] - h->box[5]) / (nz);
+    const double dx = -(h->box[0] - h->box[1]) / (nx);
+    const double dy = -(h->box[2] - h->box[3]) / (ny);
+    const long plane = (long)nx * ny;
+    cudaError_t e;
+    int t0;
+    if (pp_lp2_lpc(nx) == 0 || pp_lp2_lpc(ny) == 0 || h->rhs_complex) return PP_UNSUPPORTED;
+    // singular: no Dirichlet end anywhere (the x/y families with a zero mode
+    // are N-N or P-P)
+    const bool singular = zm && h->bc[4] != 'D' && h->bc[5] != 'D';
+    if (zm && !h->psum.p) {
+        // zero-mode column (nz) + sum of u + target mean
+        if ((e = h->psum.alloc(sizeof(double) * (nz + 2))) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+        if ((e = h->zero1.alloc(sizeof(double))) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+        if ((e = cudaMemset(h->zero1.p, 0, sizeof(double))) != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
+    }
+    float* r32 = h->out.as<float>();
+    float* A32 = h->bufA.as<float>();
+    float* B32 = h->bufB.as<float>();
+    double* u = reinterpret_cast<double*>(h->bufB.as<char>() + h->bufB.bytes / 2);
+
+    PPResidArgs ra{};
+    ra.f = h->rhs.as<double>();
+    ra.r = r32;
+    ra.psum = zm ? h->psum.as<double>() : nullptr;
+    ra.psum_scale = (kx == PP_KIND_DCT2 ? 2.0 : 1.0) * (ky == PP_KIND_DCT2 ? 2.0 : 1.0);
+    ra.nx = nx;
+    ra.ny = ny;
+    ra.nz = nz;
+    ra.dz = dz;
+    ra.Cx = (dz / dx) * (dz / dx);
+    ra.Cy = (dz / dy) * (dz / dy);
+    for (int f = 0; f < 6; ++f) ra.bc[f] = h->bc[f] == 'P' ? 2 : (h->bc[f] == 'N' ? 1 : 0);
+    ra.lift = h->liftv;
+
+    PPLinePassArgs ax{};
+    ax.n = nx;
+    ax.kind = kx;
+    ax.nlines = ny;
+    ax.nplanes = nz;
+    ax.elem_stride = 1;
+    ax.line_stride = nx;
+    ax.plane_stride = plane;
+    ax.nx = nx;
+    ax.ny = ny;
+    ax.nz = nz;
+    ax.dz = dz;
+    ax.out_scale = 1.0;
+    PPLinePassArgs ay = ax;
+    ay.n = ny;
+    ay.kind = ky;
+    ay.nlines = nx;
+    ay.elem_stride = nx;
+    ay.line_stride = 1;
+
+    PPZArgs z{};
+    z.data = reinterpret_cast<double*>(B32);
+    z.data_fp32 = 1;
+    z.skip_zero = zm ? 1 : 0;
+    z.nx = nx;
+    z.ny = ny;
+    z.nz = nz;
+    int zthreads = 0;
+    pp_zsolve_config(nz, s_cplx, nx, &z.TS, &zthreads);
+    z.tiles_x = (nx + z.TS - 1) / z.TS;
+    z.ax = h->tx.eig.as<double>();
+    z.ay = h->ty.eig.as<double>();
+    z.Cx = ra.Cx;
+    z.Cy = ra.Cy;
+    z.zlo = h->bc[4] == 'P' ? PP_Z_PERIODIC : (h->bc[4] == 'N' ? PP_Z_NEUMANN : PP_Z_DIRICHLET);
+    z.zhi = h->bc[5] == 'P' ? PP_Z_PERIODIC : (h->bc[5] == 'N' ? PP_Z_NEUMANN : PP_Z_DIRICHLET);
+    z.pin_always = 0;  // the true operator; pinned only where singular
+
+    // the kx = ky = 0 column as a 1 x 1 x nz system in FP64 (lambda = -2)
+    PPZArgs z0 = z;
+    z0.data = h->psum.as<double>();
+    z0.data_fp32 = 0;
+    z0.skip_zero = 0;
+    z0.nx = 1;
+    z0.ny = 1;
+    pp_zsolve_config(nz, false, 1, &z0.TS, &zthreads);
+    z0.tiles_x = 1;
+    z0.ax = h->zero1.as<double>();
+    z0.ay = h->zero1.as<double>();
+
+    const int sweeps = h->opt.max_sweeps < 0 ? 0 : h->opt.max_sweeps;
+    for (int sw = 0; sw <= sweeps; ++sw) {
+        const bool last = sw == sweeps;
+        t0 = stamp(h);
+        if (zm && (e = cudaMemsetAsync(h->psum.p, 0, sizeof(double) * (nz + 1), h->stream)) != cudaSuccess)
+            return set_cuda_error(h, e, PP_CUDA_ERROR);
+        ra.u = sw == 0 ? nullptr : u;
+        ra.usum = (singular && sw > 0) ? h->psum.as<double>() + nz : nullptr;
+        if ((e = pp_launch_resid(ra, h->stream)) != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
+        if (zm && (e = pp_launch_zsolve(z0, false, h->stream)) != cudaSuccess)
+            return set_cuda_error(h, e, PP_THOMAS_FAIL);
+        if (singular &&
+            (e = pp_launch_zero_mode_anchor(h->psum.as<double>(), nz, h->psum.as<double>() + nz,
+                                            h->psum.as<double>() + nz + 1, 1.0 / (ra.psum_scale * (double)nx * ny),
+                                            (double)nx * ny * nz, sw == 0, h->stream)) != cudaSuccess)
+            return set_cuda_error(h, e, PP_CUDA_ERROR);
+        stage_done(h, SLOT_RES, t0);
+
+        PPLinePassArgs a1 = ax;
+        a1.src = reinterpret_cast<const double*>(r32);
+        a1.dst = reinterpret_cast<double*>(A32);
+        t0 = stamp(h);
+        if ((e = line_pass(a1, h->tx, false, false, false, x_cplx, h->stream, true)) != cudaSuccess)
+            return set_cuda_error(h, e, PP_CUFFT_FAIL_X);
+        stage_done(h, SLOT_XF, t0);
+        PPLinePassArgs a2 = ay;
+        a2.src = reinterpret_cast<const double*>(A32);
+        a2.dst = reinterpret_cast<double*>(B32);
+        t0 = stamp(h);
+        if ((e = line_pass(a2, h->ty, false, true, x_cplx, s_cplx, h->stream, true)) != cudaSuccess)
+            return set_cuda_error(h, e, PP_CUFFT_FAIL_Y);
+        stage_done(h, SLOT_YF, t0);
+        t0 = stamp(h);
+        if ((e = pp_launch_zsolve(z, s_cplx, h->stream)) != cudaSuccess) return set_cuda_error(h, e, PP_THOMAS_FAIL);
+        stage_done(h, SLOT_Z, t0);
+        PPLinePassArgs a3 = ay;
+        a3.src = reinterpret_cast<const double*>(B32);
+        a3.dst = reinterpret_cast<double*>(A32);
+        t0 = stamp(h);
+        if ((e = line_pass(a3, h->ty, true, true, s_cplx, s_cplx, h->stream, true)) != cudaSuccess)
+            return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_Y);
+        stage_done(h, SLOT_YI, t0);
+        PPLinePassArgs a4 = ax;
+        a4.src = reinterpret_cast<const double*>(A32);
+        a4.dst = last ? h->out.as<double>() : nullptr;
+        a4.acc = u;
+        a4.acc_read = sw > 0;
+        a4.zplane = zm ? h->psum.as<double>() : nullptr;
+        a4.zscale = 1.0 / (ra.psum_scale * (double)nx * (double)ny);
+        a4.out_scale = 1. / ((double)(nx * ny));
+        t0 = stamp(h);
+        if ((e = line_pass(a4, h->tx, true, false, s_cplx, false, h->stream, true)) != cudaSuccess)
+            return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_X);
+        stage_done(h, SLOT_XI, t0);
+    }
+    h->last_sweeps = sweeps;
     return PP_SUCCESS;
 }
 
@@ -426,7 +641,9 @@ static void timing_release(pp_solver_s* h)
 {
     for (auto& e : h->tev) cudaEventDestroy(e);
     h->tev.clear();
-    h->tmax = h->tcount = 0;
+    h->trec.clear();
+    h->tmax = h->tcount = h->tnext = 0;
+    h->timing = false;
 }
 
 extern "C" {
@@ -504,6 +721,9 @@ int pp_destroy(pp_handle h)
     h->out.free();
     for (auto& b : h->lift) b.free();
     timing_release(h);
+    h->psum.free();
+    h->zero1.free();
+    h->tx.twf.free(); h->tx.csf.free(); h->ty.twf.free(); h->ty.csf.free();
     h->tx.tw.free(); h->tx.cs.free(); h->tx.eig.free();
     h->ty.tw.free(); h->ty.cs.free(); h->ty.eig.free();
     delete h;
@@ -543,7 +763,7 @@ int pp_set_options(pp_handle h, const pp_options* opt)
     if (!h) return PP_INVALID_HANDLE;
     if (!opt) return PP_INPUT_ARGS;
     if (opt->precision != PP_PRECISION_FP64 && opt->precision != PP_PRECISION_MIXED) return PP_INPUT_ARGS;
-    if (opt->precision == PP_PRECISION_MIXED) return PP_UNSUPPORTED;
+    if (opt->max_sweeps < 0 || opt->max_sweeps > 16) return PP_INPUT_ARGS;
     std::lock_guard<std::mutex> g(h->mu);
     const bool lift_changed = opt->dirichlet_lift != h->opt.dirichlet_lift;
     h->opt = *opt;
@@ -593,12 +813,11 @@ int pp_solve(pp_handle h)
     std::lock_guard<std::mutex> g(h->mu);
     if (!h->have_bc || !h->have_rhs) return PP_NOT_READY;
     cudaSetDevice(h->device);
-    if (h->tcount < h->tmax) {
-        cudaEvent_t* ev = &h->tev[(size_t)h->tcount * (PP_SOLVE_KERNELS + 1)];
-        h->tcount++;
-        return launch_solve(h, ev);
-    }
-    return launch_solve(h);
+    h->timing = h->tcount < h->tmax;
+    if (h->timing) h->tcount++;
+    const int rc = h->opt.precision == PP_PRECISION_MIXED ? launch_mixed(h) : launch_solve(h);
+    h->timing = false;
+    return rc;
 }
 
 int pp_timing_begin(pp_handle h, int max_solves)
@@ -608,7 +827,9 @@ int pp_timing_begin(pp_handle h, int max_solves)
     std::lock_guard<std::mutex> g(h->mu);
     cudaSetDevice(h->device);
     timing_release(h);
-    h->tev.resize((size_t)max_solves * (PP_SOLVE_KERNELS + 1));
+    // two events per stage; a refined solve has 6 stages per sweep
+    const int sweeps = h->opt.max_sweeps > 0 ? h->opt.max_sweeps : 0;
+    h->tev.resize((size_t)max_solves * 2 * 6 * (sweeps + 1));
     for (auto& e : h->tev)
         if (cudaEventCreate(&e) != cudaSuccess) {
             e = nullptr;
@@ -623,22 +844,20 @@ int pp_timing_begin(pp_handle h, int max_solves)
 int pp_timing_end(pp_handle h, double* kernel_ms_total, int n, int* solves)
 {
     if (!h) return PP_INVALID_HANDLE;
-    if (!kernel_ms_total || n < PP_SOLVE_KERNELS || !solves) return PP_INPUT_ARGS;
+    if (!kernel_ms_total || n < PP_SOLVE_STAGES || !solves) return PP_INPUT_ARGS;
     std::lock_guard<std::mutex> g(h->mu);
     cudaSetDevice(h->device);
-    for (int i = 0; i < PP_SOLVE_KERNELS; ++i) kernel_ms_total[i] = 0.0;
+    for (int i = 0; i < PP_SOLVE_STAGES; ++i) kernel_ms_total[i] = 0.0;
     *solves = h->tcount;
     int rc = PP_SUCCESS;
-    if (h->tcount > 0) {
-        cudaError_t e = cudaEventSynchronize(h->tev[(size_t)h->tcount * (PP_SOLVE_KERNELS + 1) - 1]);
+    if (!h->trec.empty()) {
+        cudaError_t e = cudaEventSynchronize(h->tev[h->trec.back().e1]);
         if (e != cudaSuccess) rc = set_cuda_error(h, e, PP_CUDA_ERROR);
-        for (int s = 0; s < h->tcount && rc == PP_SUCCESS; ++s) {
-            cudaEvent_t* ev = &h->tev[(size_t)s * (PP_SOLVE_KERNELS + 1)];
-            for (int i = 0; i < PP_SOLVE_KERNELS; ++i) {
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
-                kernel_ms_total[i] += ms;
-            }
+        for (const auto& r : h->trec) {
+            if (rc != PP_SUCCESS) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, h->tev[r.e0], h->tev[r.e1]);
+            kernel_ms_total[r.slot] += ms;
         }
     }
     timing_release(h);
@@ -648,25 +867,13 @@ int pp_timing_end(pp_handle h, double* kernel_ms_total, int n, int* solves)
 int pp_profile_solve(pp_handle h, double* kernel_ms, int n)
 {
     if (!h) return PP_INVALID_HANDLE;
-    if (!kernel_ms || n < PP_SOLVE_KERNELS) return PP_INPUT_ARGS;
-    std::lock_guard<std::mutex> g(h->mu);
-    if (!h->have_bc || !h->have_rhs) return PP_NOT_READY;
-    cudaSetDevice(h->device);
-    cudaEvent_t ev[PP_SOLVE_KERNELS + 1];
-    for (auto& x : ev) cudaEventCreate(&x);
-    int rc = launch_solve(h, ev);
-    cudaError_t e = cudaEventSynchronize(ev[PP_SOLVE_KERNELS]);
-    if (rc == PP_SUCCESS && e == cudaSuccess) {
-        for (int i = 0; i < PP_SOLVE_KERNELS; ++i) {
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
-            kernel_ms[i] = ms;
-        }
-    } else if (rc == PP_SUCCESS) {
-        rc = set_cuda_error(h, e, PP_CUDA_ERROR);
-    }
-    for (auto& x : ev) cudaEventDestroy(x);
-    return rc;
+    if (!kernel_ms || n < PP_SOLVE_STAGES) return PP_INPUT_ARGS;
+    int rc = pp_timing_begin(h, 1);
+    if (rc != PP_SUCCESS) return rc;
+    rc = pp_solve(h);
+    int solves = 0;
+    const int rc2 = pp_timing_end(h, kernel_ms, n, &solves);
+    return rc != PP_SUCCESS ? rc : rc2;
 }
 
 int pp_get_solution(pp_handle h, double* P)

@@ -94,10 +94,28 @@ PP_HD ZLayout zlayout(int TS, int nz, int P, bool cplx, int nthreads)
     return L;
 }
 
-template <bool CPLX>
+template <typename T>
+struct ZTo32;
+template <>
+struct ZTo32<double> {
+    using type = float;
+    static PP_D double up(float v) { return (double)v; }
+    static PP_D float down(double v) { return (float)v; }
+};
+template <>
+struct ZTo32<double2> {
+    using type = float2;
+    static PP_D double2 up(float2 v) { return make_double2(v.x, v.y); }
+    static PP_D float2 down(double2 v) { return make_float2((float)v.x, (float)v.y); }
+};
+
+// G32: the spectrum in global memory is FP32 (refined mixed-precision solve);
+// the tile and all arithmetic stay FP64
+template <bool CPLX, bool G32>
 __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
 {
     using T = typename std::conditional<CPLX, double2, double>::type;
+    using T32 = typename ZTo32<T>::type;
     extern __shared__ __align__(16) unsigned char zsm_raw[];
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int P = a.P;
@@ -117,6 +135,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     const int kx0 = (blockIdx.x - ky * a.tiles_x) * a.TS;
     const int ts = min(a.TS, nx - kx0);
     T* g = reinterpret_cast<T*>(a.data);
+    T32* g32 = reinterpret_cast<T32*>(a.data);
     const long plane = (long)nx * ny;
     const long col0 = (long)ky * nx + kx0;
 
@@ -126,10 +145,29 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     {
         const int s = threadIdx.x & (a.TS - 1);
         const int kstep = blockDim.x >> lts;
-        if (s < ts)
-            for (int k = threadIdx.x >> lts; k < nz; k += kstep)
-                if (sizeof(T) == 16) cp_async16(&tile[s * Lz.pitch + zpos(k)], &g[k * plane + col0 + s]);
-                else cp_async8(&tile[s * Lz.pitch + zpos(k)], &g[k * plane + col0 + s]);
+        if (s < ts) {
+            if (G32) {
+                // converting loads, 8 in flight per thread
+                constexpr int ZU = 8;
+                for (int k0 = threadIdx.x >> lts; k0 < nz; k0 += ZU * kstep) {
+                    T32 v[ZU];
+#pragma unroll
+                    for (int u = 0; u < ZU; ++u) {
+                        const int k = k0 + u * kstep;
+                        if (k < nz) v[u] = g32[k * plane + col0 + s];
+                    }
+#pragma unroll
+                    for (int u = 0; u < ZU; ++u) {
+                        const int k = k0 + u * kstep;
+                        if (k < nz) tile[s * Lz.pitch + zpos(k)] = ZTo32<T>::up(v[u]);
+                    }
+                }
+            } else {
+                for (int k = threadIdx.x >> lts; k < nz; k += kstep)
+                    if (sizeof(T) == 16) cp_async16(&tile[s * Lz.pitch + zpos(k)], &g[k * plane + col0 + s]);
+                    else cp_async8(&tile[s * Lz.pitch + zpos(k)], &g[k * plane + col0 + s]);
+            }
+        }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
     // interior pivots of a block, depending only on lambda: with b_0 = 1,
@@ -361,7 +399,10 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         __syncwarp(full);
 
         // ---- recover the block's rows ---------------------------------------------------
-        if (live) {
+        if (live && zero && a.skip_zero) {
+            // the kx = ky = 0 column is solved separately (in FP64 from plane sums)
+            for (int i = 0; i < M; ++i) col[zpos(s0 + i)] = zzero<T>();
+        } else if (live) {
             T xn = xl;
             col[zpos(s0 + M - 1)] = xl;
             for (int i = M - 2; i >= 1; --i) {
@@ -378,8 +419,13 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     {
         const int s = threadIdx.x & (a.TS - 1);
         const int kstep = blockDim.x >> lts;
-        if (s < ts)
-            for (int k = threadIdx.x >> lts; k < nz; k += kstep) g[k * plane + col0 + s] = tile[s * Lz.pitch + zpos(k)];
+        if (s < ts) {
+            if (G32)
+                for (int k = threadIdx.x >> lts; k < nz; k += kstep)
+                    g32[k * plane + col0 + s] = ZTo32<T>::down(tile[s * Lz.pitch + zpos(k)]);
+            else
+                for (int k = threadIdx.x >> lts; k < nz; k += kstep) g[k * plane + col0 + s] = tile[s * Lz.pitch + zpos(k)];
+        }
     }
 }
 
@@ -429,16 +475,17 @@ cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
     const size_t smem = pp_zsolve_smem(a.TS, a.nz, cplx);
     dim3 grid(a.ny * a.tiles_x), block(threads);
     cudaError_t e;
-    if (cplx) {
-        auto kfn = zsolve_kernel<true>;
-        if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-            return e;
-        kfn<<<grid, block, smem, st>>>(a);
-    } else {
-        auto kfn = zsolve_kernel<false>;
-        if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-            return e;
-        kfn<<<grid, block, smem, st>>>(a);
-    }
+#define PP_ZL(C, G)                                                                                             \
+    do {                                                                                                        \
+        auto kfn = zsolve_kernel<C, G>;                                                                         \
+        if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) \
+            return e;                                                                                           \
+        kfn<<<grid, block, smem, st>>>(a);                                                                      \
+    } while (0)
+    if (cplx && a.data_fp32) PP_ZL(true, true);
+    else if (cplx) PP_ZL(true, false);
+    else if (a.data_fp32) PP_ZL(false, true);
+    else PP_ZL(false, false);
+#undef PP_ZL
     return cudaGetLastError();
 }

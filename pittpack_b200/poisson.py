@@ -98,11 +98,13 @@ class PoissonGPU:
 
     solve = pittPack
 
+    STAGES = ("x_forward", "y_forward", "z_solve", "y_inverse", "x_inverse", "residual")
+
     def profileSolve(self) -> np.ndarray:
-        """One solve with per-kernel CUDA-event times (ms): forward x,
-        forward y, z solve, inverse y, inverse x."""
-        ms = np.zeros(5)
-        check(self._L.pp_profile_solve(self._h, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 5),
+        """One solve with per-stage CUDA-event times (ms), in the order of
+        STAGES (the residual stage exists only in the refined solve)."""
+        ms = np.zeros(6)
+        check(self._L.pp_profile_solve(self._h, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 6),
               "pp_profile_solve")
         return ms
 
@@ -110,10 +112,10 @@ class PoissonGPU:
         check(self._L.pp_timing_begin(self._h, int(max_solves)), "pp_timing_begin")
 
     def timingEnd(self):
-        """(summed ms per kernel [5], number of solves recorded)."""
-        ms = np.zeros(5)
+        """(summed ms per stage [6, order of STAGES], number of solves recorded)."""
+        ms = np.zeros(6)
         n = ctypes.c_int()
-        check(self._L.pp_timing_end(self._h, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 5,
+        check(self._L.pp_timing_end(self._h, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 6,
                                     ctypes.byref(n)), "pp_timing_end")
         return ms, n.value
 
@@ -125,6 +127,10 @@ class PoissonGPU:
             raise PittPackError(_lib.PP_INPUT_ARGS, "getSolution needs a contiguous complex128 array")
         check(self._L.pp_get_solution(self._h, out.ctypes.data), "getSolution")
         return out
+
+    def solutionToDevice(self, dptr: int) -> None:
+        """Copy P (2*nx*ny*nz doubles) to device memory at dptr, on the solver's stream."""
+        check(self._L.pp_get_solution_device(self._h, ctypes.c_void_p(dptr)), "pp_get_solution_device")
 
     def solutionDevicePtr(self) -> int:
         p = ctypes.c_void_p()

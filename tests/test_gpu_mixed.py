@@ -1,0 +1,73 @@
+"""The refined mixed-precision solve (FP32 transforms + FP64 residual
+refinement of the true 7-point system) against the FP64 oracle in exact
+zero-mode semantics.  Tolerance: relative L2 <= 1e-10, the bar of the refined
+solve, reached within 3 refinement sweeps."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def mixed_solve(nx, ny, nz, bc, f, sweeps, box=(0, 1, 0, 1, 0, 1)):
+    import pittpack_b200 as pp
+
+    with pp.make_Poisson(nx, ny, nz) as M:
+        M.assignBoundary(bc)
+        M.setBox(box)
+        M.setOptions(precision=1, max_sweeps=sweeps)
+        M.assignRhs(f)
+        M.pittPack()
+        return M.getSolution()
+
+
+def _singular(bc):
+    return bc[0:2] in ("NN", "PP") and bc[2:4] in ("NN", "PP") and bc[4] in "NP" and bc[5] in "NP"
+
+
+CASES = ["PPPPDD", "NNNNDD", "NDNDDD", "DDDDDD", "NNDDNN", "DNPPND", "PPPPPP", "NNNNNN", "DDNNPP", "PPNNDN"]
+
+
+@pytest.mark.parametrize("bc", CASES)
+@pytest.mark.parametrize("shape", [(32, 64, 24), (64, 16, 7)])
+def test_refined_vs_exact_oracle(bc, shape):
+    nx, ny, nz = shape
+    if bc[0:2] == "PP" and bc[2:4] != "PP":
+        bc = "PPPP" + bc[4:]
+    rng = np.random.default_rng(abs(hash((bc, shape))) % 2**32)
+    f = rng.uniform(-1, 1, (nz, ny, nx))
+    if _singular(bc):
+        f -= f.mean()
+    Q = O.solve(O.problem(nx, ny, nz, bc, compat_zero_mode=0), f)
+    errs = [O.rel_l2(mixed_solve(nx, ny, nz, bc, f, k).real, Q.real) for k in range(4)]
+    # every sweep reduces the error, and 3 sweeps reach the refined-solve bar
+    assert errs[0] < 1e-4, errs
+    assert errs[3] <= TOL, errs
+    assert errs[1] < errs[0], errs
+
+
+def test_refined_full_size_residual():
+    """512^3: the refined solution satisfies the 7-point system to ~FP64 accuracy."""
+    n = 512
+    bc = "NNNNDD"
+    f = np.random.default_rng(4).uniform(-1, 1, (n, n, n))
+    P = mixed_solve(n, n, n, bc, f, 2)
+    pb = O.problem(n, n, n, bc, compat_zero_mode=0)
+    b = O.scaled_rhs(pb, f)
+    r = O.residual(pb, np.ascontiguousarray(P.real), b)
+    assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(b)
+
+
+def test_refined_rejects_unsupported_inputs():
+    import pittpack_b200 as pp
+
+    with pp.make_Poisson(24, 16, 8) as M:  # 24 is not a power of two
+        M.assignBoundary("NNNNDD")
+        M.setOptions(precision=1, max_sweeps=1)
+        M.assignRhs(np.zeros((8, 16, 24)))
+        with pytest.raises(pp.PittPackError) as e:
+            M.pittPack()
+        assert e.value.code == 27
