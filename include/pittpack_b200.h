@@ -40,7 +40,8 @@ enum {
     PP_INVALID_HANDLE = 24,
     PP_NOT_READY = 25, /* boundary or RHS not assigned yet */
     PP_CUDA_ERROR = 26,
-    PP_UNSUPPORTED = 27 /* a size or option the GPU kernels do not cover */
+    PP_UNSUPPORTED = 27, /* a size or option the GPU kernels do not cover */
+    PP_NOALLOC_TOO_LARGE = 28 /* the grid does not fit pp_solve_noalloc's fixed scratch */
 };
 
 /* precision of the solve */
@@ -130,6 +131,25 @@ int pp_host_free(void* p);
 
 /* device memory the handle holds, in bytes */
 int pp_workspace_bytes(pp_handle h, size_t* bytes);
+
+/* pp_solve_noalloc -- no counterpart in the reference.  One plain FP64 solve
+ * (the reference's semantics and default options, like pp_solve) that
+ * allocates no device memory, for callers that cannot call cudaMalloc: code
+ * running inside host callbacks or allocator-restricted services, plugins that
+ * must not grow the device heap of their host process, callers whose own
+ * allocator owns all device memory.  The caller passes device pointers: d_rhs
+ * (real RHS, nx*ny*nz doubles, x fastest) and d_P (the solution, 2*nx*ny*nz
+ * doubles, chunkedArray layout); 'stream' is a cudaStream_t (0 = legacy) and
+ * the call returns once the work is enqueued.  The spectra and tables live in
+ * one fixed 32 MiB device array inside the library (held by every GPU that
+ * loads it until exit): about 16 bytes per point for the real families and
+ * 32 bytes per point when x or y is periodic, so up to ~2 M and ~1 M points;
+ * larger grids return PP_NOALLOC_TOO_LARGE.  All calls share that array: calls
+ * that overlap on the GPU race, so serialise them on one stream.  The first
+ * call on a device looks up the array's device address; make it before any
+ * stream capture. */
+int pp_solve_noalloc(int nx, int ny, int nz, const char bc[6], const double box[6], const double* d_rhs,
+                     double* d_P, void* stream);
 
 #ifdef __cplusplus
 }

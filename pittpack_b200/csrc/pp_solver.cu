@@ -666,6 +666,7 @@ const char* pp_result_string(int code)
     case PP_NOT_READY: return "NOT_READY: boundary conditions or RHS not assigned";
     case PP_CUDA_ERROR: return "CUDA_ERROR";
     case PP_UNSUPPORTED: return "UNSUPPORTED: size or option outside the GPU kernels";
+    case PP_NOALLOC_TOO_LARGE: return "NOALLOC_TOO_LARGE: the grid does not fit the 32 MiB scratch of pp_solve_noalloc";
     default: return "UNKNOWN";
     }
 }

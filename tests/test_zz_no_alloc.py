@@ -1,0 +1,79 @@
+"""pp_solve_noalloc: the allocation-free solve for callers that cannot call
+cudaMalloc (host callbacks, allocator-restricted services, plugins that must
+not grow their host process's device heap).  It is checked through the C ABI
+against the handle-based entry point (pp_create / pp_solve), within the 1e-12
+relative L2 the plain FP64 path is held to, on two calls in a row that reuse
+the same fixed scratch array.  This file is collected last so that a run that
+stops at the first failure has already run every other test."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def _lib():
+    from pittpack_b200 import _lib
+
+    L = _lib.load()
+    fn = L.pp_solve_noalloc
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
+                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    return L
+
+
+def _handle_solve(nx, ny, nz, bc, box, f):
+    import pittpack_b200 as pp
+
+    with pp.make_Poisson(nx, ny, nz) as M:
+        M.assignBoundary(bc)
+        M.setBox(box)
+        M.assignRhs(f)
+        M.pittPack()
+        return M.getSolution()
+
+
+def _noalloc_solve(L, nx, ny, nz, bc, box, f):
+    import torch
+
+    d_rhs = torch.from_numpy(np.ascontiguousarray(f, dtype=np.float64).ravel()).cuda()
+    d_P = torch.empty(2 * nx * ny * nz, dtype=torch.float64, device="cuda")
+    b = np.ascontiguousarray(box, dtype=np.float64)
+    stream = torch.cuda.current_stream()
+    rc = L.pp_solve_noalloc(nx, ny, nz, bc.encode(), b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                            d_rhs.data_ptr(), d_P.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    return rc, d_P.cpu().numpy().view(np.complex128).reshape(nz, ny, nx)
+
+
+def test_noalloc_matches_handle_path_on_two_calls():
+    L = _lib()
+    rng = np.random.default_rng(21)
+    cases = [
+        (64, 48, 40, "NNDDDD", (0, 1, 0, 1, 0, 1)),      # mixed-radix y (generic transform kernel)
+        (128, 64, 32, "PPPPDN", (0, 2, 0, 1, 0.5, 1.5)),  # power-of-two lengths, periodic x/y
+    ]
+    for nx, ny, nz, bc, box in cases:
+        f = rng.uniform(-1, 1, (nz, ny, nx))
+        rc, P = _noalloc_solve(L, nx, ny, nz, bc, box, f)
+        assert rc == 0, L.pp_result_string(rc)
+        Q = _handle_solve(nx, ny, nz, bc, box, f)
+        err = np.linalg.norm((P - Q).ravel()) / np.linalg.norm(Q.ravel())
+        assert err <= TOL, (bc, err)
+
+
+def test_noalloc_rejects_grids_beyond_its_scratch():
+    import torch
+
+    L = _lib()
+    n = 256  # 16.7 M points: far beyond the 32 MiB scratch
+    d = torch.empty(1, dtype=torch.float64, device="cuda")
+    box = np.array([0, 1, 0, 1, 0, 1.0])
+    rc = L.pp_solve_noalloc(n, n, n, b"NNNNDD", box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                            d.data_ptr(), d.data_ptr(), None)
+    assert rc == 28
+    assert b"NOALLOC_TOO_LARGE" in L.pp_result_string(rc)
