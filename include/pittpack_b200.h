@@ -49,6 +49,15 @@ enum { PP_PRECISION_FP64 = 0, PP_PRECISION_MIXED = 1 };
 
 typedef struct pp_solver_s* pp_handle;
 
+/* launch-shape choices of a handle; 0 in a field = the built-in default.  The
+ * reference has no counterpart (cuFFT plans its own launches,
+ * src/poissonGPU.cpp:5-97, and its Thomas loop is one OpenACC gang per line,
+ * src/pencilDcmp.cpp:5066-5105). */
+typedef struct {
+    int zsolve_lanes; /* lanes sharing one z system: 1..32, a power of two */
+    int line_tile;    /* lines per CTA of the generic (non-power-of-two) transform kernel, 1..32 */
+} pp_tuning;
+
 /* runtime options; the reference keeps these as compile-time switches in
  * src/include/params.h (SOLUTIONMETHOD, NITER, ...) */
 typedef struct {
@@ -90,6 +99,16 @@ int pp_assign_rhs_complex(pp_handle h, const double* rhs);
 /* RHS already on the device (real or interleaved complex); copied on the
  * handle's stream */
 int pp_assign_rhs_device(pp_handle h, const double* d_rhs, int is_complex);
+/* real host RHS copied on the handle's stream without waiting: the buffer
+ * (page-locked for a truly asynchronous copy) must stay unchanged until the
+ * stream has passed the next pp_solve.  No counterpart in the reference. */
+int pp_assign_rhs_async(pp_handle h, const double* rhs);
+/* zero copy, no counterpart in the reference: later solves read the RHS from
+ * d_rhs (real, or interleaved complex if is_complex) and write P to d_P
+ * (2*nx*ny*nz doubles), both caller-owned device memory that must outlive
+ * the binding; either may be null to keep the handle's own buffer.  A later
+ * pp_assign_rhs* call unbinds d_rhs. */
+int pp_bind_device_buffers(pp_handle h, const double* d_rhs, int is_complex, double* d_P);
 
 /* pittPack() once (src/pencilDcmp.cpp:5801-6430), asynchronous on the
  * handle's stream */
@@ -114,8 +133,12 @@ int pp_timing_end(pp_handle h, double* kernel_ms_total, int n, int* solves);
 int pp_get_solution(pp_handle h, double* P);
 /* the solution to device memory (2*nx*ny*nz doubles), on the handle's stream */
 int pp_get_solution_device(pp_handle h, double* d_P);
-/* device pointer of the handle's solution buffer (valid until pp_destroy) */
+/* device pointer of the handle's solution buffer (valid until pp_destroy),
+ * or of the bound d_P */
 int pp_solution_device_ptr(pp_handle h, const double** d_P);
+/* the solution to host memory on the handle's stream without waiting (P
+ * page-locked for a truly asynchronous copy); no counterpart in the reference */
+int pp_get_solution_async(pp_handle h, double* P);
 
 /* getError (src/pencilDcmp.cpp:2040-2208): RMS error of the solution against
  * the reference's manufactured solution; does not modify the solution */
@@ -131,6 +154,17 @@ int pp_host_free(void* p);
 
 /* device memory the handle holds, in bytes */
 int pp_workspace_bytes(pp_handle h, size_t* bytes);
+
+/* launch shapes (see pp_tuning); invalid values return PP_INPUT_ARGS */
+int pp_set_tuning(pp_handle h, const pp_tuning* t);
+int pp_get_tuning(pp_handle h, pp_tuning* t);
+/* autotuner, no counterpart in the reference: times 'reps' solves of the
+ * assigned RHS for each candidate lane count of the z solve and, when x or y
+ * is not a power of two, each line tile of the generic transform kernel
+ * (one coordinate after the other), keeps the fastest shape in the handle and
+ * reports it with its milliseconds per solve.  Synchronises the stream; the
+ * handle's solution is overwritten. */
+int pp_autotune(pp_handle h, int reps, pp_tuning* chosen, double* best_ms);
 
 /* pp_solve_noalloc -- no counterpart in the reference.  One plain FP64 solve
  * (the reference's semantics and default options, like pp_solve) that

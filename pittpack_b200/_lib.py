@@ -30,6 +30,10 @@ class Options(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("zsolve_lanes", ctypes.c_int), ("line_tile", ctypes.c_int)]
+
+
 class PittPackError(RuntimeError):
     def __init__(self, code: int, what: str):
         self.code = code
@@ -76,6 +80,12 @@ def load():
         "pp_host_alloc": ([ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)], i),
         "pp_host_free": ([ctypes.c_void_p], i),
         "pp_workspace_bytes": ([H, ctypes.POINTER(ctypes.c_size_t)], i),
+        "pp_assign_rhs_async": ([H, ctypes.c_void_p], i),
+        "pp_get_solution_async": ([H, ctypes.c_void_p], i),
+        "pp_bind_device_buffers": ([H, ctypes.c_void_p, i, ctypes.c_void_p], i),
+        "pp_set_tuning": ([H, ctypes.POINTER(Tuning)], i),
+        "pp_get_tuning": ([H, ctypes.POINTER(Tuning)], i),
+        "pp_autotune": ([H, i, ctypes.POINTER(Tuning), dp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

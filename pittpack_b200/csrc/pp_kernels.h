@@ -78,7 +78,7 @@ struct PPZArgs {
     double Cx, Cy;      // (dz/dx)^2, (dz/dy)^2
     int zlo, zhi;       // PPZBc of the two z ends
     int pin_always;     // 1: zero-mode row replacement whatever the z ends (reference)
-    int P;              // lanes per system (set by the launcher)
+    int P;              // lanes per system (0: the default for nz)
     int data_fp32;      // spectrum stored as float / float2 (solved in FP64)
     int skip_zero;      // write zeros for the kx = ky = 0 column
 };
@@ -87,6 +87,11 @@ struct PPZArgs {
 int pp_zsolve_lanes(int nz, bool cplx);
 // systems per CTA and threads per CTA of the z solve
 void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads);
+// the same for a chosen lane count (0 or invalid: the default); the launch
+// must then carry P = that lane count
+void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* threads);
+int pp_zsolve_valid_lanes(int nz, int P);
+size_t pp_zsolve_smem_p(int TS, int nz, bool cplx, int P);
 
 size_t pp_zsolve_smem(int TS, int nz, bool cplx);
 

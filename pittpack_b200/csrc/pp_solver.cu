@@ -86,6 +86,11 @@ struct pp_solver_s {
     cudaStream_t stream = 0;
     DirTables tx, ty;
     DevBuf rhs, bufA, bufB, out;
+    // caller-owned device buffers bound by pp_bind_device_buffers (zero copy):
+    // the solve reads the RHS from ext_rhs and writes P to ext_out
+    const double* ext_rhs = nullptr;
+    double* ext_out = nullptr;
+    pp_tuning tune{0, 0};  // launch-shape choices (0 = built-in default)
     DevBuf psum;   // refined solve: per-plane sums / zero-mode column (nz doubles)
     DevBuf zero1;  // one double 0.0 (eigen table of the zero-mode system)
     int last_sweeps = 0;
@@ -369,6 +374,14 @@ cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool s
     return pp_launch_line_pass(a, inverse, strided, in_cplx, out_cplx, st);
 }
 
+// lines per tile of the generic transform kernel: the tuned value when it fits
+int tuned_lines(const pp_solver_s* h, int nfft)
+{
+    const int L = h->tune.line_tile;
+    if (L >= 1 && L <= 32 && pp_line_pass_smem(L, nfft) <= 160 * 1024) return L;
+    return pick_lines(nfft);
+}
+
 int launch_solve(pp_solver_s* h)
 {
     const int nx = h->nx, ny = h->ny, nz = h->nz;
@@ -390,7 +403,7 @@ int launch_solve(pp_solver_s* h)
     ax.plane_stride = plane;
     ax.fft = h->tx.fft;
     ax.cs = h->tx.cs.as<double2>();
-    ax.L = pick_lines(ax.fft.n);
+    ax.L = tuned_lines(h, ax.fft.n);
     ax.tiles_per_plane = (ny + ax.L - 1) / ax.L;
     ax.nx = nx;
     ax.ny = ny;
@@ -406,12 +419,12 @@ int launch_solve(pp_solver_s* h)
     ay.line_stride = 1;
     ay.fft = h->ty.fft;
     ay.cs = h->ty.cs.as<double2>();
-    ay.L = pick_lines(ay.fft.n);
+    ay.L = tuned_lines(h, ay.fft.n);
     ay.tiles_per_plane = (nx + ay.L - 1) / ay.L;
 
     // forward x: rhs -> A
     PPLinePassArgs a1 = ax;
-    a1.src = h->rhs.as<double>();
+    a1.src = h->ext_rhs ? h->ext_rhs : h->rhs.as<double>();
     a1.dst = h->bufA.as<double>();
     a1.rhs_scale = 1;
     a1.lift = h->liftv;
@@ -434,7 +447,8 @@ int launch_solve(pp_solver_s* h)
     z.ny = ny;
     z.nz = nz;
     int zthreads = 0;
-    pp_zsolve_config(nz, s_cplx, nx, &z.TS, &zthreads);
+    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads);
+    z.P = h->tune.zsolve_lanes;
     z.tiles_x = (nx + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
     z.ay = h->ty.eig.as<double>();
@@ -459,7 +473,7 @@ int launch_solve(pp_solver_s* h)
     // inverse x + rescale: A -> out (always complex-interleaved)
     PPLinePassArgs a4 = ax;
     a4.src = h->bufA.as<double>();
-    a4.dst = h->out.as<double>();
+    a4.dst = h->ext_out ? h->ext_out : h->out.as<double>();
     a4.out_scale = 1. / ((double)(nx * ny));
     t0 = stamp(h);
     if ((e = line_pass(a4, h->tx, true, false, s_cplx, true, h->stream)) != cudaSuccess)
@@ -510,7 +524,7 @@ int launch_mixed(pp_solver_s* h)
     double* u = reinterpret_cast<double*>(h->bufB.as<char>() + h->bufB.bytes / 2);
 
     PPResidArgs ra{};
-    ra.f = h->rhs.as<double>();
+    ra.f = h->ext_rhs ? h->ext_rhs : h->rhs.as<double>();
     ra.r = r32;
     ra.psum = zm ? h->psum.as<double>() : nullptr;
     ra.psum_scale = (kx == PP_KIND_DCT2 ? 2.0 : 1.0) * (ky == PP_KIND_DCT2 ? 2.0 : 1.0);
@@ -551,7 +565,8 @@ int launch_mixed(pp_solver_s* h)
     z.ny = ny;
     z.nz = nz;
     int zthreads = 0;
-    pp_zsolve_config(nz, s_cplx, nx, &z.TS, &zthreads);
+    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads);
+    z.P = h->tune.zsolve_lanes;
     z.tiles_x = (nx + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
     z.ay = h->ty.eig.as<double>();
@@ -567,6 +582,7 @@ int launch_mixed(pp_solver_s* h)
     z0.data_fp32 = 0;
     z0.skip_zero = 0;
     z0.nx = 1;
+    z0.P = 0;
     z0.ny = 1;
     pp_zsolve_config(nz, false, 1, &z0.TS, &zthreads);
     z0.tiles_x = 1;
@@ -617,7 +633,7 @@ int launch_mixed(pp_solver_s* h)
         stage_done(h, SLOT_YI, t0);
         PPLinePassArgs a4 = ax;
         a4.src = reinterpret_cast<const double*>(A32);
-        a4.dst = last ? h->out.as<double>() : nullptr;
+        a4.dst = last ? (h->ext_out ? h->ext_out : h->out.as<double>()) : nullptr;
         a4.acc = u;
         a4.acc_read = sw > 0;
         a4.zplane = zm ? h->psum.as<double>() : nullptr;
@@ -798,6 +814,35 @@ static int assign_common(pp_handle h, const double* src, bool cplx, cudaMemcpyKi
     }
     h->rhs_complex = cplx;
     h->have_rhs = true;
+    h->ext_rhs = nullptr;
+    return PP_SUCCESS;
+}
+
+int pp_assign_rhs_async(pp_handle h, const double* rhs)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!rhs) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    cudaSetDevice(h->device);
+    const size_t n = (size_t)h->nx * h->ny * h->nz;
+    cudaError_t e = cudaMemcpyAsync(h->rhs.p, rhs, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
+    h->rhs_complex = false;
+    h->have_rhs = true;
+    h->ext_rhs = nullptr;
+    return PP_SUCCESS;
+}
+
+int pp_bind_device_buffers(pp_handle h, const double* d_rhs, int is_complex, double* d_P)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    std::lock_guard<std::mutex> g(h->mu);
+    if (d_rhs) {
+        h->ext_rhs = d_rhs;
+        h->rhs_complex = is_complex != 0;
+        h->have_rhs = true;
+    }
+    h->ext_out = d_P;
     return PP_SUCCESS;
 }
 
@@ -884,8 +929,21 @@ int pp_get_solution(pp_handle h, double* P)
     std::lock_guard<std::mutex> g(h->mu);
     cudaSetDevice(h->device);
     const size_t n = (size_t)h->nx * h->ny * h->nz;
-    cudaError_t e = cudaMemcpyAsync(P, h->out.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    const void* src = h->ext_out ? (const void*)h->ext_out : h->out.p;
+    cudaError_t e = cudaMemcpyAsync(P, src, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return e == cudaSuccess ? PP_SUCCESS : set_cuda_error(h, e, PP_CUDA_ERROR);
+}
+
+int pp_get_solution_async(pp_handle h, double* P)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!P) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    cudaSetDevice(h->device);
+    const size_t n = (size_t)h->nx * h->ny * h->nz;
+    const void* src = h->ext_out ? (const void*)h->ext_out : h->out.p;
+    cudaError_t e = cudaMemcpyAsync(P, src, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     return e == cudaSuccess ? PP_SUCCESS : set_cuda_error(h, e, PP_CUDA_ERROR);
 }
 
@@ -896,7 +954,9 @@ int pp_get_solution_device(pp_handle h, double* d_P)
     std::lock_guard<std::mutex> g(h->mu);
     cudaSetDevice(h->device);
     const size_t n = (size_t)h->nx * h->ny * h->nz;
-    cudaError_t e = cudaMemcpyAsync(d_P, h->out.p, 2 * n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
+    const void* src = h->ext_out ? (const void*)h->ext_out : h->out.p;
+    if (src == (const void*)d_P) return PP_SUCCESS;
+    cudaError_t e = cudaMemcpyAsync(d_P, src, 2 * n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
     return e == cudaSuccess ? PP_SUCCESS : set_cuda_error(h, e, PP_CUDA_ERROR);
 }
 
@@ -904,7 +964,7 @@ int pp_solution_device_ptr(pp_handle h, const double** d_P)
 {
     if (!h) return PP_INVALID_HANDLE;
     if (!d_P) return PP_INPUT_ARGS;
-    *d_P = h->out.as<double>();
+    *d_P = h->ext_out ? h->ext_out : h->out.as<double>();
     return PP_SUCCESS;
 }
 
@@ -996,6 +1056,101 @@ int pp_workspace_bytes(pp_handle h, size_t* bytes)
     for (auto& l : h->lift) b += l.bytes;
     b += h->tx.tw.bytes + h->tx.cs.bytes + h->tx.eig.bytes + h->ty.tw.bytes + h->ty.cs.bytes + h->ty.eig.bytes;
     *bytes = b;
+    return PP_SUCCESS;
+}
+
+static bool valid_tuning(const pp_solver_s* h, const pp_tuning* t)
+{
+    if (t->zsolve_lanes != 0 && !pp_zsolve_valid_lanes(h->nz, t->zsolve_lanes)) return false;
+    if (t->line_tile < 0 || t->line_tile > 32) return false;
+    return true;
+}
+
+int pp_set_tuning(pp_handle h, const pp_tuning* t)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!t || !valid_tuning(h, t)) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    h->tune = *t;
+    return PP_SUCCESS;
+}
+
+int pp_get_tuning(pp_handle h, pp_tuning* t)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!t) return PP_INPUT_ARGS;
+    *t = h->tune;
+    return PP_SUCCESS;
+}
+
+// milliseconds per solve of one launch shape: one untimed solve, then reps
+// solves between two events on the handle's stream
+static int time_config(pp_handle h, const pp_tuning& t, int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms)
+{
+    {
+        std::lock_guard<std::mutex> g(h->mu);
+        h->tune = t;
+    }
+    int rc = pp_solve(h);
+    if (rc != PP_SUCCESS) return rc;
+    cudaEventRecord(e0, h->stream);
+    for (int r = 0; r < reps && rc == PP_SUCCESS; ++r) rc = pp_solve(h);
+    cudaEventRecord(e1, h->stream);
+    if (rc != PP_SUCCESS) return rc;
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
+    float f = 0.f;
+    cudaEventElapsedTime(&f, e0, e1);
+    *ms = f / reps;
+    return PP_SUCCESS;
+}
+
+int pp_autotune(pp_handle h, int reps, pp_tuning* chosen, double* best_ms)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (reps < 1 || reps > 100) return PP_INPUT_ARGS;
+    if (!h->have_bc || !h->have_rhs) return PP_NOT_READY;
+    cudaSetDevice(h->device);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        return PP_CUDA_ERROR;
+    }
+    const pp_tuning start = h->tune;
+    pp_tuning best{0, 0};
+    double bms = 0.0;
+    int rc = time_config(h, best, reps, e0, e1, &bms);
+    // z solve: lane counts around the default
+    for (int P = 1; P <= 32 && rc == PP_SUCCESS; P *= 2) {
+        if (!pp_zsolve_valid_lanes(h->nz, P)) continue;
+        pp_tuning t = best;
+        t.zsolve_lanes = P;
+        double ms = 0.0;
+        rc = time_config(h, t, reps, e0, e1, &ms);
+        if (rc == PP_SUCCESS && ms < bms) {
+            bms = ms;
+            best = t;
+        }
+    }
+    // generic transform kernel: lines per tile, only where it runs
+    const bool generic = pp_lp2_lpc(h->nx) == 0 || pp_lp2_lpc(h->ny) == 0;
+    for (int L = 1; generic && L <= 32 && rc == PP_SUCCESS; L *= 2) {
+        pp_tuning t = best;
+        t.line_tile = L;
+        double ms = 0.0;
+        rc = time_config(h, t, reps, e0, e1, &ms);
+        if (rc == PP_SUCCESS && ms < bms) {
+            bms = ms;
+            best = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> g(h->mu);
+    h->tune = rc == PP_SUCCESS ? best : start;
+    if (rc != PP_SUCCESS) return rc;
+    if (chosen) *chosen = best;
+    if (best_ms) *best_ms = bms;
     return PP_SUCCESS;
 }
 

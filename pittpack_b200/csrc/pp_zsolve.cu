@@ -174,13 +174,14 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     // b_1 = lambda, b_i = lambda b_{i-1} - b_{i-2} (Chebyshev U_i(lambda/2)),
     //   gamma_i = b_{i-1} / b_i,  alpha_i = (-1)^{i-1} / b_i,
     // the same numbers as the Thomas recurrence gamma_i = 1 / (lambda - gamma_{i-1}).
-    // One thread per system; the divisions are independent.  For |lambda| > 1e3
-    // the b_i could overflow, so the division recurrence is used instead.
+    // One thread per system; the divisions are independent.  |b_i| grows like
+    // |lambda|^i, so where mm log2|lambda| could leave the double range the
+    // division recurrence is used instead.
     for (int s = threadIdx.x; s < ts; s += blockDim.x) {
         const double lam = (-2.0 + a.ax[kx0 + s] * a.Cx) + a.ay[ky] * a.Cy;
         double2* tb = reinterpret_cast<double2*>(zsm_raw + Lz.tab_off) + (size_t)s * Lz.mmax;
         const int mm = Lz.mmax;
-        if (fabs(lam) <= 1.0e3) {
+        if ((double)mm * log2(fabs(lam) + 1.0) < 900.0) {
             double bm = 1.0, bc = lam, sg = 1.0;
             for (int i = 1; i < mm; ++i) {
                 tb[i] = make_double2(bm / bc, sg / bc);
@@ -460,19 +461,42 @@ void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads)
 
 size_t pp_zsolve_smem(int TS, int nz, bool cplx)
 {
-    const int P = pp_zsolve_lanes(nz, cplx);
+    return pp_zsolve_smem_p(TS, nz, cplx, pp_zsolve_lanes(nz, cplx));
+}
+
+// a lane count the kernel accepts: a power of two <= 32 leaving every lane at
+// least two rows
+int pp_zsolve_valid_lanes(int nz, int P)
+{
+    return P >= 1 && P <= 32 && (P & (P - 1)) == 0 && (P == 1 || P <= nz / 2);
+}
+
+size_t pp_zsolve_smem_p(int TS, int nz, bool cplx, int P)
+{
     const int th = TS * P < 32 ? 32 : TS * P;
     return zlayout(TS, nz, P, cplx, th).bytes;
+}
+
+// the launch shape for a chosen lane count (0 or invalid: the default)
+void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* threads)
+{
+    const int P = pp_zsolve_valid_lanes(nz, lanes) ? lanes : pp_zsolve_lanes(nz, cplx);
+    int ts = PP_Z_THREADS / P;
+    while (ts > 1 && pp_zsolve_smem_p(ts, nz, cplx, P) > 112 * 1024) ts >>= 1;
+    while (ts > 1 && ts > nx) ts >>= 1;
+    *TS = ts;
+    *threads = ts * P < 32 ? 32 : ts * P;
 }
 
 cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
 {
     if (a0.nz < 3 || a0.nz > PP_Z_MAX_NZ) return cudaErrorInvalidValue;
     PPZArgs a = a0;
-    a.P = pp_zsolve_lanes(a.nz, cplx);
+    if (!pp_zsolve_valid_lanes(a.nz, a.P)) a.P = pp_zsolve_lanes(a.nz, cplx);
     const int threads = a.TS * a.P < 32 ? 32 : a.TS * a.P;
     if (threads > PP_Z_THREADS) return cudaErrorInvalidValue;
-    const size_t smem = pp_zsolve_smem(a.TS, a.nz, cplx);
+    const size_t smem = pp_zsolve_smem_p(a.TS, a.nz, cplx, a.P);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
     dim3 grid(a.ny * a.tiles_x), block(threads);
     cudaError_t e;
 #define PP_ZL(C, G)                                                                                             \

@@ -142,6 +142,42 @@ class PoissonGPU:
         check(self._L.pp_get_error_manufactured(self._h, ctypes.byref(e)), "getError")
         return e.value
 
+    # -- zero copy, asynchronous copies, launch shapes --------------------------
+    def bindDeviceBuffers(self, d_rhs: int = 0, is_complex: bool = False, d_P: int = 0) -> None:
+        """Solve straight from / into caller-owned device buffers (pointers as
+        ints, 0 keeps the handle's own buffer)."""
+        check(self._L.pp_bind_device_buffers(self._h, ctypes.c_void_p(d_rhs or None), int(bool(is_complex)),
+                                             ctypes.c_void_p(d_P or None)), "pp_bind_device_buffers")
+
+    def assignRhsAsync(self, rhs: np.ndarray) -> None:
+        """Real RHS copied on the handle's stream without waiting; keep rhs
+        alive and unchanged until the stream has passed the next solve."""
+        assert rhs.dtype == np.float64 and rhs.flags.c_contiguous and rhs.size == self.nx * self.ny * self.nz
+        check(self._L.pp_assign_rhs_async(self._h, rhs.ctypes.data), "pp_assign_rhs_async")
+
+    def getSolutionAsync(self, out: np.ndarray) -> None:
+        """Solution copied into out (complex128, nx*ny*nz) on the handle's
+        stream without waiting; synchronize() before reading it."""
+        assert out.dtype == np.complex128 and out.flags.c_contiguous and out.size == self.nx * self.ny * self.nz
+        check(self._L.pp_get_solution_async(self._h, out.ctypes.data), "pp_get_solution_async")
+
+    def setTuning(self, zsolve_lanes: int = 0, line_tile: int = 0) -> None:
+        t = _lib.Tuning(int(zsolve_lanes), int(line_tile))
+        check(self._L.pp_set_tuning(self._h, ctypes.byref(t)), "pp_set_tuning")
+
+    def tuning(self):
+        t = _lib.Tuning()
+        check(self._L.pp_get_tuning(self._h, ctypes.byref(t)), "pp_get_tuning")
+        return {"zsolve_lanes": t.zsolve_lanes, "line_tile": t.line_tile}
+
+    def autotune(self, reps: int = 3):
+        """Time candidate launch shapes on the assigned RHS and keep the
+        fastest; returns (shape dict, ms per solve)."""
+        t = _lib.Tuning()
+        ms = ctypes.c_double()
+        check(self._L.pp_autotune(self._h, int(reps), ctypes.byref(t), ctypes.byref(ms)), "pp_autotune")
+        return {"zsolve_lanes": t.zsolve_lanes, "line_tile": t.line_tile}, ms.value
+
     def setStream(self, stream_ptr: int) -> None:
         check(self._L.pp_set_stream(self._h, ctypes.c_void_p(stream_ptr)), "pp_set_stream")
 
