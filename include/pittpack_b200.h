@@ -166,6 +166,56 @@ int pp_get_tuning(pp_handle h, pp_tuning* t);
  * handle's solution is overwritten. */
 int pp_autotune(pp_handle h, int reps, pp_tuning* chosen, double* best_ms);
 
+/* ---- batched solves (no counterpart in the reference, which solves one grid
+ * per PencilDcmp object, src/main.cpp:73-134): many grids of uneven sizes and
+ * boundary conditions, each bound zero-copy to caller device buffers, solved
+ * by one CUDA-graph launch ----------------------------------------------- */
+typedef struct {
+    int nx, ny, nz;
+    char bc[6];
+    double box[6];
+    const double* d_rhs; /* device, real, nx*ny*nz doubles */
+    double* d_P;         /* device, 2*nx*ny*nz doubles (chunkedArray layout) */
+} pp_batch_item;
+typedef struct pp_batch_s* pp_batch;
+/* builds one handle per grid (options 'opt', or the defaults if null),
+ * autotunes each size class once when 'autotune' is set, solves every grid
+ * once and captures all solves into one graph whose 'branches' streams run
+ * concurrently; on the current device */
+int pp_batch_create(const pp_batch_item* items, int n, const pp_options* opt, int branches, int autotune,
+                    pp_batch* out);
+/* one launch of the captured graph on 'stream' (cudaStream_t as void*) */
+int pp_batch_run(pp_batch b, void* stream);
+/* number of grids and of graph nodes */
+int pp_batch_info(pp_batch b, int* grids, int* graph_nodes);
+int pp_batch_destroy(pp_batch b);
+
+/* ---- request server (no counterpart in the reference): single solves
+ * arriving over time, continuously batched on the current GPU -------------- */
+typedef struct {
+    int nx, ny, nz;
+    char bc[6];
+    double box[6];
+    int precision;     /* PP_PRECISION_FP64, or PP_PRECISION_MIXED (refined) */
+    int sweeps;        /* refinement sweeps of the mixed mode */
+    const double* rhs; /* host, real, nx*ny*nz doubles; page-locked for overlap */
+    double* P;         /* host, 2*nx*ny*nz doubles, written when the request completes */
+} pp_request;
+typedef struct pp_server_s* pp_server;
+/* 'streams' requests can be on the GPU at once; handles (plans, twiddles and
+ * workspaces) are kept per shape within hbm_fraction of the free device
+ * memory at creation, idle ones evicted least recently used */
+int pp_server_create(int streams, double hbm_fraction, pp_server* out);
+/* queue a request (the buffers must stay valid until pp_server_wait returns) */
+int pp_server_submit(pp_server s, const pp_request* r, unsigned long long* ticket);
+/* wait for a request: its status, latency (submit to solution in host
+ * memory, ms) and the precision it ran in */
+int pp_server_wait(pp_server s, unsigned long long ticket, double* latency_ms, int* precision);
+/* requests completed, most requests on the GPU at once, bytes of pooled handles */
+int pp_server_stats(pp_server s, long long* completed, int* max_inflight, size_t* pool_bytes);
+/* finishes queued requests, then frees everything */
+int pp_server_destroy(pp_server s);
+
 /* pp_solve_noalloc -- no counterpart in the reference.  One plain FP64 solve
  * (the reference's semantics and default options, like pp_solve) that
  * allocates no device memory, for callers that cannot call cudaMalloc: code
