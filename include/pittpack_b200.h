@@ -63,8 +63,7 @@ typedef struct {
 typedef struct {
     int precision;        /* PP_PRECISION_FP64 (default) or PP_PRECISION_MIXED: FP32
                              transforms + FP64 iterative refinement of the true
-                             7-point system (exact zero mode); real RHS and
-                             power-of-two nx, ny */
+                             7-point system (exact zero mode); real RHS */
     int max_sweeps;       /* refinement sweeps after the first FP32 solve (0..16) */
     double tolerance;     /* target the caller checks; sweeps are a fixed count (no host sync) */
     int compat_zero_mode; /* 1 (default): reference zero-mode row replacement, src/triDiag.cpp:1753-1776 */

@@ -28,3 +28,35 @@ PP_D double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 PP_D double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 // multiply by i*s (s = +1 or -1)
 PP_D double2 cmul_i(double2 a, double s) { return make_double2(-s * a.y, s * a.x); }
+
+// ---- complex helpers for float2 / double2 ------------------------------------
+template <typename C>
+struct CReal;
+template <>
+struct CReal<double2> {
+    using type = double;
+};
+template <>
+struct CReal<float2> {
+    using type = float;
+};
+
+template <typename C>
+PP_D C mkc(typename CReal<C>::type x, typename CReal<C>::type y)
+{
+    C r;
+    r.x = x;
+    r.y = y;
+    return r;
+}
+template <typename C>
+PP_D C c_add(C a, C b) { return mkc<C>(a.x + b.x, a.y + b.y); }
+template <typename C>
+PP_D C c_sub(C a, C b) { return mkc<C>(a.x - b.x, a.y - b.y); }
+template <typename C>
+PP_D C c_mul(C a, C b) { return mkc<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <typename C>
+PP_D C c_scale(C a, typename CReal<C>::type s) { return mkc<C>(a.x * s, a.y * s); }
+// multiply by SIGN * i
+template <int SIGN, typename C>
+PP_D C c_mul_si(C a) { return SIGN > 0 ? mkc<C>(-a.y, a.x) : mkc<C>(a.y, -a.x); }

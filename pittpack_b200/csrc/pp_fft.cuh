@@ -1,4 +1,5 @@
-// Batched mixed-radix (2,3,4,5,8) Stockham FFT on lines held in shared memory.
+// Batched mixed-radix (2,3,4,5,8) Stockham FFT on lines held in shared memory,
+// in FP64 (double2) or FP32 (float2).
 //
 // The reference hands every line to FFTW or cuFFT (src/poissonCPU.cpp:40-234,
 // src/poissonGPU.cpp:5-97: unnormalised, exp(-2 pi i jk/N) forward and
@@ -22,88 +23,92 @@ struct PPFftPlan {
     const double2* tw;           // W_n^m = exp(-2 pi i m / n), m < n
 };
 
-// r-point DFT in registers; SIGN = -1 forward, +1 backward
-template <int SIGN>
-PP_D void dft2(double2* v)
+// r-point DFTs in registers; SIGN = -1 forward, +1 backward
+template <int SIGN, typename C>
+PP_D void dft2(C* v)
 {
-    double2 a = v[0], b = v[1];
-    v[0] = cadd(a, b);
-    v[1] = csub(a, b);
+    C a = v[0], b = v[1];
+    v[0] = c_add(a, b);
+    v[1] = c_sub(a, b);
 }
 
-template <int SIGN>
-PP_D void dft3(double2* v)
+template <int SIGN, typename C>
+PP_D void dft3(C* v)
 {
-    const double h = 0.86602540378443864676372317075293618;  // sin(2 pi / 3)
-    double2 t1 = cadd(v[1], v[2]);
-    double2 t2 = csub(v[1], v[2]);
-    double2 m = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
-    double2 r = cmul_i(cscale(t2, h), (double)SIGN);
-    v[0] = cadd(v[0], t1);
-    v[1] = cadd(m, r);
-    v[2] = csub(m, r);
+    using R = typename CReal<C>::type;
+    const R h = (R)0.86602540378443864676372317075293618;  // sin(2 pi / 3)
+    C t1 = c_add(v[1], v[2]);
+    C t2 = c_sub(v[1], v[2]);
+    C m = mkc<C>(v[0].x - (R)0.5 * t1.x, v[0].y - (R)0.5 * t1.y);
+    C r = c_mul_si<SIGN>(c_scale(t2, h));
+    v[0] = c_add(v[0], t1);
+    v[1] = c_add(m, r);
+    v[2] = c_sub(m, r);
 }
 
-template <int SIGN>
-PP_D void dft4(double2* v)
+template <int SIGN, typename C>
+PP_D void dft4(C* v)
 {
-    double2 a = cadd(v[0], v[2]);
-    double2 b = csub(v[0], v[2]);
-    double2 c = cadd(v[1], v[3]);
-    double2 d = cmul_i(csub(v[1], v[3]), (double)SIGN);
-    v[0] = cadd(a, c);
-    v[2] = csub(a, c);
-    v[1] = cadd(b, d);
-    v[3] = csub(b, d);
+    C a = c_add(v[0], v[2]);
+    C b = c_sub(v[0], v[2]);
+    C c = c_add(v[1], v[3]);
+    C d = c_mul_si<SIGN>(c_sub(v[1], v[3]));
+    v[0] = c_add(a, c);
+    v[2] = c_sub(a, c);
+    v[1] = c_add(b, d);
+    v[3] = c_sub(b, d);
 }
 
-template <int SIGN>
-PP_D void dft5(double2* v)
+template <int SIGN, typename C>
+PP_D void dft5(C* v)
 {
-    const double c1 = 0.30901699437494742410229341718281906;   // cos(2 pi / 5)
-    const double c2 = -0.80901699437494742410229341718281906;  // cos(4 pi / 5)
-    const double s1 = 0.95105651629515357211643933337938214;   // sin(2 pi / 5)
-    const double s2 = 0.58778525229247312916870595463907277;   // sin(4 pi / 5)
-    double2 t1 = cadd(v[1], v[4]);
-    double2 t2 = cadd(v[2], v[3]);
-    double2 t3 = csub(v[1], v[4]);
-    double2 t4 = csub(v[2], v[3]);
-    double2 a1 = make_double2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
-    double2 a2 = make_double2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
-    double2 b1 = cmul_i(make_double2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y), (double)SIGN);
-    double2 b2 = cmul_i(make_double2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y), (double)SIGN);
-    v[0] = cadd(v[0], cadd(t1, t2));
-    v[1] = cadd(a1, b1);
-    v[4] = csub(a1, b1);
-    v[2] = cadd(a2, b2);
-    v[3] = csub(a2, b2);
+    using R = typename CReal<C>::type;
+    const R c1 = (R)0.30901699437494742410229341718281906;   // cos(2 pi / 5)
+    const R c2 = (R)-0.80901699437494742410229341718281906;  // cos(4 pi / 5)
+    const R s1 = (R)0.95105651629515357211643933337938214;   // sin(2 pi / 5)
+    const R s2 = (R)0.58778525229247312916870595463907277;   // sin(4 pi / 5)
+    C t1 = c_add(v[1], v[4]);
+    C t2 = c_add(v[2], v[3]);
+    C t3 = c_sub(v[1], v[4]);
+    C t4 = c_sub(v[2], v[3]);
+    C a1 = mkc<C>(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+    C a2 = mkc<C>(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+    C b1 = c_mul_si<SIGN>(mkc<C>(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y));
+    C b2 = c_mul_si<SIGN>(mkc<C>(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y));
+    v[0] = c_add(v[0], c_add(t1, t2));
+    v[1] = c_add(a1, b1);
+    v[4] = c_sub(a1, b1);
+    v[2] = c_add(a2, b2);
+    v[3] = c_sub(a2, b2);
 }
 
-template <int SIGN>
-PP_D void dft8(double2* v)
+template <int SIGN, typename C>
+PP_D void dft8(C* v)
 {
-    const double h = 0.70710678118654752440084436210484904;  // sqrt(2) / 2
-    double2 e[4] = {v[0], v[2], v[4], v[6]};
-    double2 o[4] = {v[1], v[3], v[5], v[7]};
+    using R = typename CReal<C>::type;
+    const R h = (R)0.70710678118654752440084436210484904;  // sqrt(2) / 2
+    C e[4] = {v[0], v[2], v[4], v[6]};
+    C o[4] = {v[1], v[3], v[5], v[7]};
     dft4<SIGN>(e);
     dft4<SIGN>(o);
     // o[k] *= exp(SIGN 2 pi i k / 8)
-    double2 o1 = make_double2(h * (o[1].x - SIGN * o[1].y), h * (o[1].y + SIGN * o[1].x));
-    double2 o2 = cmul_i(o[2], (double)SIGN);
-    double2 o3 = make_double2(h * (-o[3].x - SIGN * o[3].y), h * (-o[3].y + SIGN * o[3].x));
-    v[0] = cadd(e[0], o[0]);
-    v[4] = csub(e[0], o[0]);
-    v[1] = cadd(e[1], o1);
-    v[5] = csub(e[1], o1);
-    v[2] = cadd(e[2], o2);
-    v[6] = csub(e[2], o2);
-    v[3] = cadd(e[3], o3);
-    v[7] = csub(e[3], o3);
+    const R s = (R)SIGN;
+    C o1 = mkc<C>(h * (o[1].x - s * o[1].y), h * (o[1].y + s * o[1].x));
+    C o2 = c_mul_si<SIGN>(o[2]);
+    C o3 = mkc<C>(h * (-o[3].x - s * o[3].y), h * (-o[3].y + s * o[3].x));
+    v[0] = c_add(e[0], o[0]);
+    v[4] = c_sub(e[0], o[0]);
+    v[1] = c_add(e[1], o1);
+    v[5] = c_sub(e[1], o1);
+    v[2] = c_add(e[2], o2);
+    v[6] = c_sub(e[2], o2);
+    v[3] = c_add(e[3], o3);
+    v[7] = c_sub(e[3], o3);
 }
 
-template <int R, int SIGN>
-PP_D void stockham_pass(const double2* __restrict__ src, double2* __restrict__ dst, int n, int nlines, int ns,
-                        const double2* __restrict__ tw, int tid, int nthreads)
+template <int R, int SIGN, typename C>
+PP_D void stockham_pass(const C* __restrict__ src, C* __restrict__ dst, int n, int nlines, int ns,
+                        const C* __restrict__ tw, int tid, int nthreads)
 {
     const int nb = n / R;         // butterflies per line
     const int tstride = n / (ns * R);
@@ -112,17 +117,17 @@ PP_D void stockham_pass(const double2* __restrict__ src, double2* __restrict__ d
         const int l = t / nb;
         const int j = t - l * nb;
         const int k = j % ns;
-        const double2* in = src + l * n;
-        double2* out = dst + l * n;
-        double2 v[R];
+        const C* in = src + l * n;
+        C* out = dst + l * n;
+        C v[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = in[j + q * nb];
         if (ns > 1) {
 #pragma unroll
             for (int q = 1; q < R; ++q) {
-                double2 w = __ldg(&tw[q * k * tstride]);
+                C w = __ldg(&tw[q * k * tstride]);
                 if (SIGN > 0) w.y = -w.y;
-                v[q] = cmul(v[q], w);
+                v[q] = c_mul(v[q], w);
             }
         }
         if (R == 2) dft2<SIGN>(v);
@@ -137,26 +142,27 @@ PP_D void stockham_pass(const double2* __restrict__ src, double2* __restrict__ d
 }
 
 // Transform nlines lines of plan.n points held in a (line-major); b is scratch
-// of the same size.  Returns the buffer that holds the result.  Ends with a
-// __syncthreads(); must be entered by every thread of the block after the
-// data in 'a' is complete (the caller synchronises before the call).
-template <int SIGN>
-__device__ double2* fft_lines(double2* a, double2* b, int nlines, const PPFftPlan& P, int tid, int nthreads)
+// of the same size; tw is the plan's twiddle table in the precision of C.
+// Returns the buffer that holds the result.  Ends with a __syncthreads(); must
+// be entered by every thread of the block after the data in 'a' is complete
+// (the caller synchronises before the call).
+template <int SIGN, typename C>
+__device__ C* fft_lines(C* a, C* b, int nlines, const PPFftPlan& P, const C* tw, int tid, int nthreads)
 {
-    double2* src = a;
-    double2* dst = b;
+    C* src = a;
+    C* dst = b;
     int ns = 1;
     for (int p = 0; p < P.npass; ++p) {
         const int r = P.radix[p];
         switch (r) {
-        case 2: stockham_pass<2, SIGN>(src, dst, P.n, nlines, ns, P.tw, tid, nthreads); break;
-        case 3: stockham_pass<3, SIGN>(src, dst, P.n, nlines, ns, P.tw, tid, nthreads); break;
-        case 4: stockham_pass<4, SIGN>(src, dst, P.n, nlines, ns, P.tw, tid, nthreads); break;
-        case 5: stockham_pass<5, SIGN>(src, dst, P.n, nlines, ns, P.tw, tid, nthreads); break;
-        default: stockham_pass<8, SIGN>(src, dst, P.n, nlines, ns, P.tw, tid, nthreads); break;
+        case 2: stockham_pass<2, SIGN>(src, dst, P.n, nlines, ns, tw, tid, nthreads); break;
+        case 3: stockham_pass<3, SIGN>(src, dst, P.n, nlines, ns, tw, tid, nthreads); break;
+        case 4: stockham_pass<4, SIGN>(src, dst, P.n, nlines, ns, tw, tid, nthreads); break;
+        case 5: stockham_pass<5, SIGN>(src, dst, P.n, nlines, ns, tw, tid, nthreads); break;
+        default: stockham_pass<8, SIGN>(src, dst, P.n, nlines, ns, tw, tid, nthreads); break;
         }
         __syncthreads();
-        double2* t = src;
+        C* t = src;
         src = dst;
         dst = t;
         ns *= r;

@@ -42,7 +42,8 @@ struct PPLinePassArgs {
     PPLift lift;
     int nx, ny, nz;
     double out_scale;  // inverse x-pass: 1 / (nx ny)
-    // used by the power-of-two kernel (pp_linepass_pow2.cu)
+    // twiddles in the kernel's precision: used by the power-of-two kernel
+    // (pp_linepass_pow2.cu) and by the FP32 generic kernel
     const void* tw;    // FFT twiddles (double2 or float2), length n or n/2
     const void* cs2;   // family twiddles in the kernel's precision
     int in_cplx, out_cplx;
@@ -55,15 +56,19 @@ struct PPLinePassArgs {
     int acc_read;       // 0: the previous u is zero (first sweep), acc is not read
 };
 
-size_t pp_line_pass_smem(int L, int nfft);
+// shared memory of the generic kernel: two buffers of L lines of nfft complex
+// points in FP64, or in FP32 (fp32)
+size_t pp_line_pass_smem(int L, int nfft, bool fp32 = false);
 // power-of-two lengths 16..2048: complex FFT lines per CTA (0 = not covered);
 // a tile holds this many data lines for the periodic family and twice as many
 // for the real families
 int pp_lp2_lpc(int n);
 template <typename Real, typename TI, typename TO>
 cudaError_t pp_launch_line_pass_pow2(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st);
+// generic 2/3/5-smooth lengths; fp32: the FP32 kernel, twiddles from a.tw and
+// a.cs2 (FP64: a.fft.tw and a.cs), with the refinement epilogue when a.acc is set
 cudaError_t pp_launch_line_pass(const PPLinePassArgs& a, bool inverse, bool strided, bool in_cplx, bool out_cplx,
-                                cudaStream_t st);
+                                cudaStream_t st, bool fp32 = false);
 
 // z-boundary kinds of the tridiagonal systems
 enum PPZBc : int { PP_Z_DIRICHLET = 0, PP_Z_NEUMANN = 1, PP_Z_PERIODIC = 2 };

@@ -32,11 +32,27 @@
 //           the sign of odd outputs.
 // The DCT/DST families read only the real part of their input, as the
 // reference's pre-processing does.
+//
+// The kernel runs in FP64 (the plain solve) or FP32 (the correction solves of
+// the refined mixed-precision mode, for lengths the power-of-two kernel does
+// not cover).  In FP32 the inverse x pass ends in the refinement epilogue:
+// u = u_prev + v / (nx ny) + zero-mode constant, accumulated in FP64.
 #include "pp_common.cuh"
 #include "pp_fft.cuh"
 #include "pp_kernels.h"
 
 namespace {
+
+template <typename R>
+struct Vec2T;
+template <>
+struct Vec2T<double> {
+    using type = double2;
+};
+template <>
+struct Vec2T<float> {
+    using type = float2;
+};
 
 // Makhoul even/odd position: where input element e goes (and, inverse, where
 // output element e is read from)
@@ -55,16 +71,29 @@ PP_D double lift_at(const PPLift& L, int i, int j, int k, int nx, int ny, int nz
     return s;
 }
 
-template <bool INVERSE, bool STRIDED, bool IN_CPLX, bool OUT_CPLX>
+template <typename R, bool INVERSE, bool STRIDED, bool IN_CPLX, bool OUT_CPLX>
 __global__ void __launch_bounds__(PP_LINE_THREADS) line_pass_kernel(PPLinePassArgs a)
 {
-    extern __shared__ double2 smem[];
+    using C = typename Vec2T<R>::type;
+    extern __shared__ __align__(16) unsigned char pp_lp_smem[];
+    C* smem = reinterpret_cast<C*>(pp_lp_smem);
     const int n = a.n;
     const int kind = a.kind;
     const bool quarter = pp_kind_is_quarter(kind);
     const int nf = a.fft.n;  // n, or n/2 for the quarter-wave families
     const int tid = threadIdx.x;
     const int nth = blockDim.x;
+    // FFT and family twiddles in the kernel's precision
+    const C* tw;
+    const C* cs;
+    if constexpr (sizeof(R) == 8) {
+        tw = reinterpret_cast<const C*>(a.fft.tw);
+        cs = reinterpret_cast<const C*>(a.cs);
+    } else {
+        tw = reinterpret_cast<const C*>(a.tw);
+        cs = reinterpret_cast<const C*>(a.cs2);
+    }
+    const R* src = reinterpret_cast<const R*>(a.src);
 
     const int tile = blockIdx.x;
     const int plane = tile / a.tiles_per_plane;
@@ -72,9 +101,9 @@ __global__ void __launch_bounds__(PP_LINE_THREADS) line_pass_kernel(PPLinePassAr
     const int nl = min(a.L, a.nlines - l0);
     const long base = (long)plane * a.plane_stride + (long)l0 * a.line_stride;
 
-    double2* bufA = smem;
-    double2* bufB = smem + (size_t)a.L * nf;
-    double* stage = reinterpret_cast<double*>(bufB);  // raw real lines, n per line
+    C* bufA = smem;
+    C* bufB = smem + (size_t)a.L * nf;
+    R* stage = reinterpret_cast<R*>(bufB);  // raw real lines, n per line
 
     const bool staged = quarter || (INVERSE && kind != PP_KIND_FFT);
 
@@ -90,15 +119,15 @@ __global__ void __launch_bounds__(PP_LINE_THREADS) line_pass_kernel(PPLinePassAr
             e = idx - l * n;
         }
         const long off = base + (long)l * a.line_stride + (long)e * a.elem_stride;
-        double2 v;
-        if (IN_CPLX) v = reinterpret_cast<const double2*>(a.src)[off];
-        else v = make_double2(a.src[off], 0.0);
+        C v;
+        if (IN_CPLX) v = reinterpret_cast<const C*>(src)[off];
+        else v = mkc<C>(src[off], (R)0);
         if (a.rhs_scale) {
-            v.x = v.x * a.dz * a.dz;
-            v.y = v.y * a.dz * a.dz;
+            v.x = v.x * (R)a.dz * (R)a.dz;
+            v.y = v.y * (R)a.dz * (R)a.dz;
             if (a.lift.any) {
                 // forward x-pass: line index = y index j, plane = z index k
-                v.x = v.x - lift_at(a.lift, e, l0 + l, plane, a.nx, a.ny, a.nz);
+                v.x = v.x - (R)lift_at(a.lift, e, l0 + l, plane, a.nx, a.ny, a.nz);
             }
         }
         if (kind == PP_KIND_FFT) {
@@ -106,11 +135,11 @@ __global__ void __launch_bounds__(PP_LINE_THREADS) line_pass_kernel(PPLinePassAr
         } else if (!staged) {
             // forward DCT-II / DST-II: reorder straight into the FFT input
             if (kind == PP_KIND_DCT2) {
-                bufA[l * nf + makhoul_pos(e, n)] = make_double2(v.x, 0.0);
+                bufA[l * nf + makhoul_pos(e, n)] = mkc<C>(v.x, (R)0);
             } else {  // DST-II: x'[j] = (-1)^j x[n-1-j]
                 const int j = n - 1 - e;
-                const double s = (j & 1) ? -1.0 : 1.0;
-                bufA[l * nf + makhoul_pos(j, n)] = make_double2(s * v.x, 0.0);
+                const R s = (j & 1) ? (R)-1 : (R)1;
+                bufA[l * nf + makhoul_pos(j, n)] = mkc<C>(s * v.x, (R)0);
             }
         } else {
             // stage the real part (reversed / sign-swapped where the family says)
@@ -132,23 +161,23 @@ __global__ void __launch_bounds__(PP_LINE_THREADS) line_pass_kernel(PPLinePassAr
         for (int idx = tid; idx < tot2; idx += nth) {
             const int l = idx / nf;
             const int k = idx - l * nf;
-            const double* X = stage + l * n;
-            double2 V;
+            const R* X = stage + l * n;
+            C V;
             if (quarter) {
-                const double2 w = __ldg(&a.cs[k]);  // e^{-i pi k / n}
-                const double xa = X[2 * k], xb = X[n - 1 - 2 * k];
-                V = make_double2(xa * w.x - xb * w.y, xa * w.y + xb * w.x);
+                const C w = __ldg(&cs[k]);  // e^{-i pi k / n}
+                const R xa = X[2 * k], xb = X[n - 1 - 2 * k];
+                V = mkc<C>(xa * w.x - xb * w.y, xa * w.y + xb * w.x);
             } else if (k == 0) {
-                V = make_double2(0.5 * 1.0 * X[0], 0.0);
+                V = mkc<C>((R)0.5 * X[0], (R)0);
             } else if (k <= n / 2) {
-                const double2 t = __ldg(&a.cs[k]);  // (cos t_k, sin t_k)
-                V.y = 0.5 * (t.y * X[k] - t.x * X[n - k]);
-                V.x = 0.5 * (t.x * X[k] + t.y * X[n - k]);
+                const C t = __ldg(&cs[k]);  // (cos t_k, sin t_k)
+                V.y = (R)0.5 * (t.y * X[k] - t.x * X[n - k]);
+                V.x = (R)0.5 * (t.x * X[k] + t.y * X[n - k]);
             } else {
                 const int kk = n - k;
-                const double2 t = __ldg(&a.cs[kk]);
-                V.y = -(0.5 * (t.y * X[kk] - t.x * X[n - kk]));
-                V.x = 0.5 * (t.x * X[kk] + t.y * X[n - kk]);
+                const C t = __ldg(&cs[kk]);
+                V.y = -((R)0.5 * (t.y * X[kk] - t.x * X[n - kk]));
+                V.x = (R)0.5 * (t.x * X[kk] + t.y * X[n - kk]);
             }
             bufA[l * nf + k] = V;
         }
@@ -157,8 +186,8 @@ __global__ void __launch_bounds__(PP_LINE_THREADS) line_pass_kernel(PPLinePassAr
 
     // ---- 3. FFT --------------------------------------------------------------
     const bool backward = INVERSE && !quarter;
-    double2* res = backward ? fft_lines<+1>(bufA, bufB, nl, a.fft, tid, nth)
-                            : fft_lines<-1>(bufA, bufB, nl, a.fft, tid, nth);
+    C* res = backward ? fft_lines<+1>(bufA, bufB, nl, a.fft, tw, tid, nth)
+                      : fft_lines<-1>(bufA, bufB, nl, a.fft, tw, tid, nth);
 
     // ---- 4. post-processing and store ---------------------------------------
     for (int idx = tid; idx < total; idx += nth) {
@@ -170,72 +199,75 @@ __global__ void __launch_bounds__(PP_LINE_THREADS) line_pass_kernel(PPLinePassAr
             l = idx / n;
             e = idx - l * n;
         }
-        const double2* R = res + l * nf;
-        double2 o;
+        const C* Rl = res + l * nf;
+        C o;
         if (kind == PP_KIND_FFT) {
-            o = R[e];
+            o = Rl[e];
         } else if (quarter) {
             const int k = e;
-            int p;
-            double v;
-            if ((k & 1) == 0) {
-                p = k >> 1;
-            } else {
-                p = (n - 1 - k) >> 1;
-            }
-            const double2 w = __ldg(&a.cs[nf + p]);  // e^{-i pi (4p+1)/(4n)}
-            const double2 z = R[p];
-            const double wr = z.x * w.x - z.y * w.y;
-            const double wi = z.x * w.y + z.y * w.x;
-            v = ((k & 1) == 0) ? wr : -wi;
-            v *= INVERSE ? 1.0 : 2.0;
+            const int p = (k & 1) == 0 ? (k >> 1) : ((n - 1 - k) >> 1);
+            const C w = __ldg(&cs[nf + p]);  // e^{-i pi (4p+1)/(4n)}
+            const C z = Rl[p];
+            const R wr = z.x * w.x - z.y * w.y;
+            const R wi = z.x * w.y + z.y * w.x;
+            R v = ((k & 1) == 0) ? wr : -wi;
+            v *= INVERSE ? (R)1 : (R)2;
             if (kind == PP_KIND_DST4 && (k & 1)) v = -v;
-            o = make_double2(v, 0.0);
+            o = mkc<C>(v, (R)0);
         } else if (!INVERSE) {
             // DCT-II value at k, optionally through the DST swap
             int k = e;
-            double sgn = 1.0;
+            R sgn = 1;
             if (kind == PP_KIND_DST2) {
-                sgn = (e & 1) ? -1.0 : 1.0;
+                sgn = (e & 1) ? (R)-1 : (R)1;
                 k = n - 1 - e;
             }
-            double2 V;
+            C V;
             if (k > n / 2) {
-                V = R[n - k];
+                V = Rl[n - k];
                 V.y = -V.y;
             } else {
-                V = R[k];
+                V = Rl[k];
             }
-            const double2 t = __ldg(&a.cs[k]);
-            o = make_double2(sgn * (2. * (V.x * t.x + V.y * t.y)), 0.0);
+            const C t = __ldg(&cs[k]);
+            o = mkc<C>(sgn * ((R)2. * (V.x * t.x + V.y * t.y)), (R)0);
         } else {
             // DCT-III output reorder, optionally through the DST swap
             if (kind == PP_KIND_DST2) {
                 const int j = n - 1 - e;
-                const double s = (e & 1) ? -1.0 : 1.0;
-                o = make_double2(s * R[makhoul_pos(j, n)].x, 0.0);
+                const R s = (e & 1) ? (R)-1 : (R)1;
+                o = mkc<C>(s * Rl[makhoul_pos(j, n)].x, (R)0);
             } else {
-                o = make_double2(R[makhoul_pos(e, n)].x, 0.0);
+                o = mkc<C>(Rl[makhoul_pos(e, n)].x, (R)0);
             }
         }
-        if (a.out_scale != 1.0) {
-            o.x = a.out_scale * o.x;
-            o.y = a.out_scale * o.y;
-        }
         const long off = base + (long)l * a.line_stride + (long)e * a.elem_stride;
-        if (OUT_CPLX) reinterpret_cast<double2*>(a.dst)[off] = o;
-        else a.dst[off] = o.x;
+        if (a.acc) {
+            // u = u_prev + scale * correction + zero-mode constant, in FP64
+            const double u = (a.acc_read ? a.acc[off] : 0.0) + a.out_scale * (double)o.x +
+                             (a.zplane ? a.zscale * a.zplane[plane] : 0.0);
+            if (a.dst) reinterpret_cast<double2*>(a.dst)[off] = make_double2(u, 0.0);
+            else a.acc[off] = u;
+            continue;
+        }
+        if (a.out_scale != 1.0) {
+            o.x = (R)a.out_scale * o.x;
+            o.y = (R)a.out_scale * o.y;
+        }
+        R* dst = reinterpret_cast<R*>(a.dst);
+        if (OUT_CPLX) reinterpret_cast<C*>(dst)[off] = o;
+        else dst[off] = o.x;
     }
 }
 
-template <bool INVERSE, bool STRIDED>
+template <typename R, bool INVERSE, bool STRIDED>
 cudaError_t launch_typed(const PPLinePassArgs& a, bool in_cplx, bool out_cplx, size_t smem, cudaStream_t st)
 {
     dim3 grid(a.nplanes * a.tiles_per_plane);
     dim3 block(PP_LINE_THREADS);
 #define PP_LAUNCH(IC, OC)                                                                                   \
     do {                                                                                                    \
-        auto kfn = line_pass_kernel<INVERSE, STRIDED, IC, OC>;                                             \
+        auto kfn = line_pass_kernel<R, INVERSE, STRIDED, IC, OC>;                                          \
         cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
         if (e != cudaSuccess) return e;                                                                     \
         kfn<<<grid, block, smem, st>>>(a);                                                                  \
@@ -248,18 +280,29 @@ cudaError_t launch_typed(const PPLinePassArgs& a, bool in_cplx, bool out_cplx, s
 #undef PP_LAUNCH
 }
 
+template <typename R>
+cudaError_t launch_prec(const PPLinePassArgs& a, bool inverse, bool strided, bool in_cplx, bool out_cplx,
+                        cudaStream_t st)
+{
+    const size_t smem = pp_line_pass_smem(a.L, a.fft.n, sizeof(R) == 4);
+    if (inverse) {
+        return strided ? launch_typed<R, true, true>(a, in_cplx, out_cplx, smem, st)
+                       : launch_typed<R, true, false>(a, in_cplx, out_cplx, smem, st);
+    }
+    return strided ? launch_typed<R, false, true>(a, in_cplx, out_cplx, smem, st)
+                   : launch_typed<R, false, false>(a, in_cplx, out_cplx, smem, st);
+}
+
 }  // namespace
 
-size_t pp_line_pass_smem(int L, int nfft) { return 2 * (size_t)L * nfft * sizeof(double2); }
+size_t pp_line_pass_smem(int L, int nfft, bool fp32)
+{
+    return 2 * (size_t)L * nfft * (fp32 ? sizeof(float2) : sizeof(double2));
+}
 
 cudaError_t pp_launch_line_pass(const PPLinePassArgs& a, bool inverse, bool strided, bool in_cplx, bool out_cplx,
-                                cudaStream_t st)
+                                cudaStream_t st, bool fp32)
 {
-    const size_t smem = pp_line_pass_smem(a.L, a.fft.n);
-    if (inverse) {
-        return strided ? launch_typed<true, true>(a, in_cplx, out_cplx, smem, st)
-                       : launch_typed<true, false>(a, in_cplx, out_cplx, smem, st);
-    }
-    return strided ? launch_typed<false, true>(a, in_cplx, out_cplx, smem, st)
-                   : launch_typed<false, false>(a, in_cplx, out_cplx, smem, st);
+    return fp32 ? launch_prec<float>(a, inverse, strided, in_cplx, out_cplx, st)
+                : launch_prec<double>(a, inverse, strided, in_cplx, out_cplx, st);
 }

@@ -344,14 +344,29 @@ void stage_done(pp_solver_s* h, int slot, int i0)
 }
 enum { SLOT_XF = 0, SLOT_YF = 1, SLOT_Z = 2, SLOT_YI = 3, SLOT_XI = 4, SLOT_RES = 5 };
 
+// lines per CTA tile of the FP32 generic kernel (same 64 KB rule)
+int pick_lines_fp32(int nfft)
+{
+    int L = 16;
+    while (L > 1 && pp_line_pass_smem(L, nfft, true) > 64 * 1024) L >>= 1;
+    return L;
+}
+
 // one transform pass: the register-resident kernel for power-of-two lengths,
 // the generic shared-memory Stockham kernel otherwise
 cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool strided, bool in_cplx,
                       bool out_cplx, cudaStream_t st, bool fp32 = false)
 {
     const int lpc = pp_lp2_lpc(d.n);
+    if (fp32 && lpc == 0) {
+        a.fft = d.fft;
+        a.tw = d.twf.p;
+        a.cs2 = d.csf.p;
+        a.L = pick_lines_fp32(d.fft.n);
+        a.tiles_per_plane = (a.nlines + a.L - 1) / a.L;
+        return pp_launch_line_pass(a, inverse, strided, in_cplx, out_cplx, st, true);
+    }
     if (fp32) {
-        if (lpc == 0) return cudaErrorInvalidValue;
         a.tw = d.twf.p;
         a.cs2 = d.csf.p;
         a.in_cplx = in_cplx;
@@ -508,7 +523,7 @@ int launch_mixed(pp_solver_s* h)
     const long plane = (long)nx * ny;
     cudaError_t e;
     int t0;
-    if (pp_lp2_lpc(nx) == 0 || pp_lp2_lpc(ny) == 0 || h->rhs_complex) return PP_UNSUPPORTED;
+    if (h->rhs_complex) return PP_UNSUPPORTED;
     // singular: no Dirichlet end anywhere (the x/y families with a zero mode
     // are N-N or P-P)
     const bool singular = zm && h->bc[4] != 'D' && h->bc[5] != 'D';

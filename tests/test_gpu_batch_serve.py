@@ -113,5 +113,5 @@ def test_server_rejects_a_request_that_never_fits():
     rhs[...] = 1.0
     P = pinned_empty((16, 16, 16), np.complex128)
     st, _, _ = S.wait(S.submit(16, 16, 16, "DDDDDD", rhs, P))
-    assert st == 2  # ALLOCATION_FAIL
+    assert st == 15  # ALLOCATION_FAIL
     S.close()

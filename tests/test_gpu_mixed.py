@@ -32,7 +32,9 @@ CASES = ["PPPPDD", "NNNNDD", "NDNDDD", "DDDDDD", "NNDDNN", "DNPPND", "PPPPPP", "
 
 
 @pytest.mark.parametrize("bc", CASES)
-@pytest.mark.parametrize("shape", [(32, 64, 24), (64, 16, 7)])
+# power-of-two lengths (register-resident FP32 kernel) and 2/3/5-smooth ones
+# (shared-memory FP32 kernel), mixed within one grid too
+@pytest.mark.parametrize("shape", [(32, 64, 24), (64, 16, 7), (48, 40, 30), (24, 20, 18), (60, 36, 9), (32, 30, 16)])
 def test_refined_vs_exact_oracle(bc, shape):
     nx, ny, nz = shape
     if bc[0:2] == "PP" and bc[2:4] != "PP":
@@ -64,10 +66,10 @@ def test_refined_full_size_residual():
 def test_refined_rejects_unsupported_inputs():
     import pittpack_b200 as pp
 
-    with pp.make_Poisson(24, 16, 8) as M:  # 24 is not a power of two
+    with pp.make_Poisson(24, 16, 8) as M:  # the refined solve takes a real RHS only
         M.assignBoundary("NNNNDD")
         M.setOptions(precision=1, max_sweeps=1)
-        M.assignRhs(np.zeros((8, 16, 24)))
+        M.assignRhsComplex(np.zeros((8, 16, 24), dtype=np.complex128))
         with pytest.raises(pp.PittPackError) as e:
             M.pittPack()
         assert e.value.code == 27
