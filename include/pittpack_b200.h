@@ -46,6 +46,11 @@ enum {
 
 /* precision of the solve */
 enum { PP_PRECISION_FP64 = 0, PP_PRECISION_MIXED = 1 };
+/* z solver of the plain FP64 solve: the direct partition-method / PCR solve
+ * (default; the reference's Thomas path, src/pencilDcmp.cpp:5066-5105), or
+ * multigrid V-cycles on the same systems (the reference's alternate
+ * MultiGrid solver, src/multiGrid.cpp:1105-1515) */
+enum { PP_ZSOLVE_DIRECT = 0, PP_ZSOLVE_MULTIGRID = 1 };
 
 typedef struct pp_solver_s* pp_handle;
 
@@ -68,6 +73,7 @@ typedef struct {
     double tolerance;     /* target the caller checks; sweeps are a fixed count (no host sync) */
     int compat_zero_mode; /* 1 (default): reference zero-mode row replacement, src/triDiag.cpp:1753-1776 */
     int dirichlet_lift;   /* 1 (default): reference modifyRhsDirichlet, src/pencilDcmp.cpp:4623-4835 */
+    int z_solver;         /* PP_ZSOLVE_DIRECT (default) or PP_ZSOLVE_MULTIGRID (plain FP64 solve only) */
 } pp_options;
 
 /* the reference's PittPackGetErrorEnum (src/pencilDcmp.cpp:4869-4913) */
@@ -142,6 +148,11 @@ int pp_get_solution_async(pp_handle h, double* P);
 /* getError (src/pencilDcmp.cpp:2040-2208): RMS error of the solution against
  * the reference's manufactured solution; does not modify the solution */
 int pp_get_error_manufactured(pp_handle h, double* err);
+/* multigrid z solver: the most V-cycles any system of the last solve took,
+ * and how many systems stopped at the cycle bound above 1e-10 relative
+ * residual (waits for the handle's stream); no counterpart in the reference,
+ * whose MultiGrid prints its residuals (src/multiGrid.cpp:1415-1515) */
+int pp_zsolve_stats(pp_handle h, int* max_cycles, int* unconverged);
 
 /* CUDA stream for the handle's work (cudaStream_t passed as void*); 0 = legacy */
 int pp_set_stream(pp_handle h, void* stream);

@@ -18,6 +18,8 @@ PP_NOT_READY = 25
 PP_UNSUPPORTED = 27
 PP_PRECISION_FP64 = 0
 PP_PRECISION_MIXED = 1
+PP_ZSOLVE_DIRECT = 0
+PP_ZSOLVE_MULTIGRID = 1
 
 
 class Options(ctypes.Structure):
@@ -27,6 +29,7 @@ class Options(ctypes.Structure):
         ("tolerance", ctypes.c_double),
         ("compat_zero_mode", ctypes.c_int),
         ("dirichlet_lift", ctypes.c_int),
+        ("z_solver", ctypes.c_int),
     ]
 
 
@@ -75,6 +78,7 @@ def load():
         "pp_get_solution_device": ([H, ctypes.c_void_p], i),
         "pp_solution_device_ptr": ([H, ctypes.POINTER(ctypes.c_void_p)], i),
         "pp_get_error_manufactured": ([H, dp], i),
+        "pp_zsolve_stats": ([H, ctypes.POINTER(i), ctypes.POINTER(i)], i),
         "pp_set_stream": ([H, ctypes.c_void_p], i),
         "pp_synchronize": ([H], i),
         "pp_host_alloc": ([ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)], i),

@@ -119,3 +119,23 @@ cudaError_t pp_launch_resid(const PPResidArgs& a, cudaStream_t st);
 cudaError_t pp_launch_zero_mode_anchor(double* zcol, int nz, const double* usum, double* mstar, double zscale,
                                        double npts, int first, cudaStream_t st);
 cudaError_t pp_launch_zsolve(const PPZArgs& a, bool cplx, cudaStream_t st);
+
+// alternate z solve by multigrid V-cycles (pp_zsolve_mg.cu): the same systems
+// as pp_launch_zsolve, FP64 spectra
+struct PPZMgArgs {
+    double* data;       // spectrum [k][ky][kx], real or complex
+    int nx, ny, nz;
+    const double* ax;
+    const double* ay;
+    double Cx, Cy;
+    int zlo, zhi;
+    int pin_always;
+    int max_cycles;     // bound on V-cycles per system
+    int* stats;         // [0] max cycles used, [1] systems stopped at the bound; or null
+    int G;              // systems per CTA (set by the launcher)
+    int tot;            // cells of all levels (set by the launcher)
+};
+int pp_zsolve_mg_levels_total(int nz);
+size_t pp_zsolve_mg_smem(int G, int nz, bool cplx);
+// cudaErrorInvalidValue when one system's levels do not fit shared memory
+cudaError_t pp_launch_zsolve_mg(PPZMgArgs a, bool cplx, cudaStream_t st);

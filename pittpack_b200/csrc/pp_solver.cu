@@ -93,6 +93,7 @@ struct pp_solver_s {
     pp_tuning tune{0, 0};  // launch-shape choices (0 = built-in default)
     DevBuf psum;   // refined solve: per-plane sums / zero-mode column (nz doubles)
     DevBuf zero1;  // one double 0.0 (eigen table of the zero-mode system)
+    DevBuf mgstats;  // multigrid z solve: max cycles, unconverged systems (2 ints)
     int last_sweeps = 0;
     DevBuf lift[6];
     PPLift liftv{};
@@ -475,7 +476,31 @@ int launch_solve(pp_solver_s* h)
     z.zhi = h->bc[5] == 'P' ? PP_Z_PERIODIC : (h->bc[5] == 'N' ? PP_Z_NEUMANN : PP_Z_DIRICHLET);
     z.pin_always = h->opt.compat_zero_mode ? 1 : 0;
     t0 = stamp(h);
-    if ((e = pp_launch_zsolve(z, s_cplx, h->stream)) != cudaSuccess) return set_cuda_error(h, e, PP_THOMAS_FAIL);
+    if (h->opt.z_solver == PP_ZSOLVE_MULTIGRID) {
+        if (!h->mgstats.p && (e = h->mgstats.alloc(2 * sizeof(int))) != cudaSuccess)
+            return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+        if ((e = cudaMemsetAsync(h->mgstats.p, 0, 2 * sizeof(int), h->stream)) != cudaSuccess)
+            return set_cuda_error(h, e, PP_CUDA_ERROR);
+        PPZMgArgs m{};
+        m.data = z.data;
+        m.nx = nx;
+        m.ny = ny;
+        m.nz = nz;
+        m.ax = z.ax;
+        m.ay = z.ay;
+        m.Cx = z.Cx;
+        m.Cy = z.Cy;
+        m.zlo = z.zlo;
+        m.zhi = z.zhi;
+        m.pin_always = z.pin_always;
+        m.max_cycles = 60;
+        m.stats = h->mgstats.as<int>();
+        e = pp_launch_zsolve_mg(m, s_cplx, h->stream);
+        if (e == cudaErrorInvalidValue) return PP_UNSUPPORTED;  // levels exceed shared memory
+        if (e != cudaSuccess) return set_cuda_error(h, e, PP_THOMAS_FAIL);
+    } else if ((e = pp_launch_zsolve(z, s_cplx, h->stream)) != cudaSuccess) {
+        return set_cuda_error(h, e, PP_THOMAS_FAIL);
+    }
     stage_done(h, SLOT_Z, t0);
     // inverse y: B -> A
     PPLinePassArgs a3 = ay;
@@ -523,7 +548,7 @@ int launch_mixed(pp_solver_s* h)
     const long plane = (long)nx * ny;
     cudaError_t e;
     int t0;
-    if (h->rhs_complex) return PP_UNSUPPORTED;
+    if (h->rhs_complex || h->opt.z_solver != PP_ZSOLVE_DIRECT) return PP_UNSUPPORTED;
     // singular: no Dirichlet end anywhere (the x/y families with a zero mode
     // are N-N or P-P)
     const bool singular = zm && h->bc[4] != 'D' && h->bc[5] != 'D';
@@ -710,6 +735,7 @@ int pp_default_options(pp_options* opt)
     opt->tolerance = 1e-10;
     opt->compat_zero_mode = 1;
     opt->dirichlet_lift = 1;
+    opt->z_solver = PP_ZSOLVE_DIRECT;
     return PP_SUCCESS;
 }
 
@@ -755,6 +781,7 @@ int pp_destroy(pp_handle h)
     timing_release(h);
     h->psum.free();
     h->zero1.free();
+    h->mgstats.free();
     h->tx.twf.free(); h->tx.csf.free(); h->ty.twf.free(); h->ty.csf.free();
     h->tx.tw.free(); h->tx.cs.free(); h->tx.eig.free();
     h->ty.tw.free(); h->ty.cs.free(); h->ty.eig.free();
@@ -796,6 +823,7 @@ int pp_set_options(pp_handle h, const pp_options* opt)
     if (!opt) return PP_INPUT_ARGS;
     if (opt->precision != PP_PRECISION_FP64 && opt->precision != PP_PRECISION_MIXED) return PP_INPUT_ARGS;
     if (opt->max_sweeps < 0 || opt->max_sweeps > 16) return PP_INPUT_ARGS;
+    if (opt->z_solver != PP_ZSOLVE_DIRECT && opt->z_solver != PP_ZSOLVE_MULTIGRID) return PP_INPUT_ARGS;
     std::lock_guard<std::mutex> g(h->mu);
     const bool lift_changed = opt->dirichlet_lift != h->opt.dirichlet_lift;
     h->opt = *opt;
@@ -803,6 +831,24 @@ int pp_set_options(pp_handle h, const pp_options* opt)
         cudaSetDevice(h->device);
         return build_lift(h);
     }
+    return PP_SUCCESS;
+}
+
+int pp_zsolve_stats(pp_handle h, int* max_cycles, int* unconverged)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!max_cycles || !unconverged) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    *max_cycles = 0;
+    *unconverged = 0;
+    if (!h->mgstats.p) return PP_SUCCESS;
+    cudaSetDevice(h->device);
+    int v[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(v, h->mgstats.p, sizeof(v), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
+    *max_cycles = v[0];
+    *unconverged = v[1];
     return PP_SUCCESS;
 }
 

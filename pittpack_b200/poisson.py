@@ -142,6 +142,13 @@ class PoissonGPU:
         check(self._L.pp_get_error_manufactured(self._h, ctypes.byref(e)), "getError")
         return e.value
 
+    def zsolveStats(self):
+        """Multigrid z solver: (most V-cycles of any system, systems stopped
+        at the cycle bound above 1e-10) for the last solve."""
+        c, u = ctypes.c_int(), ctypes.c_int()
+        check(self._L.pp_zsolve_stats(self._h, ctypes.byref(c), ctypes.byref(u)), "pp_zsolve_stats")
+        return c.value, u.value
+
     # -- zero copy, asynchronous copies, launch shapes --------------------------
     def bindDeviceBuffers(self, d_rhs: int = 0, is_complex: bool = False, d_P: int = 0) -> None:
         """Solve straight from / into caller-owned device buffers (pointers as
