@@ -16,10 +16,17 @@ is the faster mode that meets rel err <= 1e-10; both are in `modes`.
 Metric: Mpoints/s = grid points solved / time.
 
 `value` times the solves with the RHS already resident in HBM (CUDA events on
-the solver stream, max over ranks); `e2e` times the public API end to end per
-solve: pinned host RHS -> pp_assign_rhs (H2D) -> pp_solve -> pp_get_solution
-(D2H of the complex-interleaved solution).  Inputs (1 GiB per grid) are larger
-than the 126 MB L2, so no flush is needed between solves.
+the solver stream, max over ranks); `e2e` times the public API end to end:
+per grid, page-locked host RHS -> pp_assign_rhs_async (H2D) -> pp_solve ->
+pp_get_solution_async (D2H of the complex-interleaved solution), the four
+grids on four streams so that their copies overlap, wall clock until every
+stream has finished.  Inputs (1 GiB per grid) are larger than the 126 MB L2,
+so no flush is needed between solves.
+
+Two more workloads are reported beside the headline (skip with --no-batch /
+--no-serve): `batch`, 96 uneven grids (seed 7) solved by one CUDA-graph
+replay in both precisions, and `serving`, Poisson-arrival request streams
+(seed 11, 100..5000 req/s) through the request server with p50/p99 latency.
 
 Multi-GPU: the solve does not shard (one grid per GPU); N ranks run N
 independent replicas of the workload and `value` counts the points of all.
@@ -178,6 +185,178 @@ def make_rhs(torch, bc: str, n: int, seed: int, device):
     gn = torch.Generator(device=device).manual_seed(seed + 1000)
     f.add_((torch.rand(f.shape, generator=gn, dtype=torch.float64, device=device) * 2 - 1) * 1e-3)
     return f
+
+
+# ---- batched and served workloads ---------------------------------------------
+BATCH_XY = [32, 48, 64, 96, 128, 160, 192]
+XY_FAMILIES = ["PPPP", "NNNN", "NDND", "DDDD"]
+SERVE_RATES = [100, 500, 1000, 2000, 5000]
+
+
+def _singular(bc: str) -> bool:
+    return all(bc[k:k + 2] in ("PP", "NN") for k in (0, 2, 4))
+
+
+def batch_grids(seed: int = 7, count: int = 96):
+    """96 grids: nx, ny from {32..192} (2/3/5-smooth), nz uniform in [32, 256],
+    x/y family uniform over the four, z Dirichlet or Neumann at both ends."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nx = int(rng.choice(BATCH_XY))
+        ny = int(rng.choice(BATCH_XY))
+        nz = int(rng.integers(32, 257))
+        bc = XY_FAMILIES[int(rng.integers(0, 4))] + ("DD", "NN")[int(rng.integers(0, 2))]
+        out.append((nx, ny, nz, bc))
+    return out
+
+
+def smooth_even(v: float) -> int:
+    """Nearest even 2/3/5-smooth integer to v (>= 16)."""
+    best = None
+    for n in range(16, 4 * int(v) + 32, 2):
+        m = n
+        for p in (2, 3, 5):
+            while m % p == 0:
+                m //= p
+        if m == 1 and (best is None or abs(n - v) < abs(best - v)):
+            best = n
+        if best is not None and n > v and n - v > abs(best - v):
+            break
+    return best
+
+
+def serve_requests(seed: int, count: int):
+    """Cubic grids with log-uniform edge in [32, 384] (so n^3 between 32^3 and
+    384^3), rounded to even 2/3/5-smooth lengths; x/y family uniform; z Dirichlet."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    req = []
+    for _ in range(count):
+        n = smooth_even(float(np.exp(rng.uniform(np.log(32), np.log(384)))))
+        req.append((n, XY_FAMILIES[int(rng.integers(0, 4))] + "DD"))
+    return req
+
+
+def run_batch_leg(args, torch, stream):
+    """One CUDA-graph replay solves all 96 grids; Mpoints/s = sum of points /
+    replay time (CUDA events on the launching stream).  Both modes use the
+    exact zero mode; the refined batch's error is taken against the FP64 batch."""
+    from pittpack_b200.batch import Batch
+
+    grids = batch_grids()
+    items, bufs, total = [], [], 0
+    for k, (nx, ny, nz, bc) in enumerate(grids):
+        g = torch.Generator(device="cuda").manual_seed(7000 + k)
+        f = torch.randn((nz, ny, nx), dtype=torch.float64, device="cuda", generator=g)
+        if _singular(bc):
+            f -= f.mean()
+        P = torch.empty(2 * f.numel(), dtype=torch.float64, device="cuda")
+        items.append(dict(nx=nx, ny=ny, nz=nz, bc=bc, d_rhs=f.data_ptr(), d_P=P.data_ptr()))
+        bufs.append((f, P))
+        total += f.numel()
+    res, ref = {}, None
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        B = Batch(items, precision=prec, sweeps=args.sweeps, compat_zero_mode=0, branches=8, autotune=True)
+        for _ in range(max(3, args.warmup)):
+            B.run(stream.cuda_stream)
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        reps = max(3, args.steps)
+        t0.record(stream)
+        for _ in range(reps):
+            B.run(stream.cuda_stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / reps
+        _, nodes = B.info()
+        res[name] = {"value": total / (ms / 1e3) / 1e6, "ms_per_batch": ms, "graph_nodes": nodes}
+        if prec == 0:
+            ref = [P[0::2].clone() for _, P in bufs]
+        else:
+            errs = [float(torch.linalg.norm(P[0::2] - r) / torch.linalg.norm(r)) for (_, P), r in zip(bufs, ref)]
+            res[name]["max_rel_err_vs_fp64"] = max(errs)
+        B.close()
+    best = "mixed" if (res["mixed"]["value"] > res["fp64"]["value"]
+                       and res["mixed"]["max_rel_err_vs_fp64"] <= 1e-10) else "fp64"
+    del bufs, ref
+    torch.cuda.empty_cache()
+    return {"workload": "96 grids (seed 7): nx, ny in {32,48,64,96,128,160,192}, nz U[32,256], "
+                        "x/y family uniform, z DD or NN, RHS N(0,1) zero-mean where singular; one graph replay",
+            "grids": len(grids), "points": total, "unit": "Mpoints/s", "value": res[best]["value"],
+            "mode": best, "modes": res}
+
+
+def run_serve_leg(args):
+    """Poisson arrivals of single solves (seed 11) at each rate; host RHS in
+    page-locked memory -> server (H2D, solve, D2H on one of 8 streams) -> host
+    solution.  Latency is counted from the scheduled arrival, so time a request
+    waits on the client side (at most 10 outstanding) is included."""
+    import numpy as np
+
+    from pittpack_b200.batch import Server
+    from pittpack_b200.poisson import pinned_empty
+
+    count = args.serve_requests
+    reqs = serve_requests(11, count)
+    nmax = max(n for n, _ in reqs)
+    rng = np.random.default_rng(11)
+    rhs = pinned_empty((nmax ** 3,), np.float64)
+    rhs[...] = rng.standard_normal(nmax ** 3)
+    ring = [pinned_empty((nmax ** 3,), np.complex128) for _ in range(10)]
+    pts = sum(n ** 3 for n, _ in reqs)
+    out = {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        S = Server(streams=8, hbm_fraction=0.5)
+        # plans, twiddles and workspaces resident before the stream starts
+        seen = set()
+        for n, bc in reqs:
+            if (n, bc) not in seen:
+                seen.add((n, bc))
+                st, _, _ = S.wait(S.submit(n, n, n, bc, rhs[:n ** 3], ring[0][:n ** 3], precision=prec,
+                                           sweeps=args.sweeps))
+                if st != 0:
+                    raise RuntimeError(f"warm-up request {n}^3 {bc} failed with status {st}")
+        per_rate = []
+        for rate in SERVE_RATES:
+            arr = np.cumsum(np.random.default_rng(11 + rate).exponential(1.0 / rate, count))
+            tickets, t_sub = [], []
+            lat, ends, used = [0.0] * count, [0.0] * count, [0] * count
+            t0 = time.perf_counter()
+
+            def collect(i):
+                st, ms, pu = S.wait(tickets[i])
+                if st != 0:
+                    raise RuntimeError(f"request {i} failed with status {st}")
+                lat[i] = (t_sub[i] - (t0 + arr[i])) * 1e3 + ms
+                ends[i] = t_sub[i] + ms / 1e3
+                used[i] = pu
+
+            for i, (n, bc) in enumerate(reqs):
+                while time.perf_counter() < t0 + arr[i]:
+                    pass
+                if i >= len(ring):
+                    collect(i - len(ring))
+                t_sub.append(time.perf_counter())
+                tickets.append(S.submit(n, n, n, bc, rhs[:n ** 3], ring[i % len(ring)][:n ** 3],
+                                        precision=prec, sweeps=args.sweeps))
+            for i in range(max(0, count - len(ring)), count):
+                collect(i)
+            span = max(ends) - t0
+            per_rate.append({"rate_req_s": rate, "p50_ms": float(np.percentile(lat, 50)),
+                             "p99_ms": float(np.percentile(lat, 99)), "throughput_req_s": count / span,
+                             "Mpoints_s": pts / span / 1e6, "refined_fraction": sum(used) / count})
+        st = S.stats()
+        S.close()
+        out[name] = {"per_rate": per_rate, "max_inflight": st["max_inflight"]}
+    return {"workload": f"{count} requests per rate (seed 11), cubic grids with log-uniform edge 32..384 "
+                        "rounded to even 2/3/5-smooth, x/y family uniform, z DD, RHS N(0,1); 8 streams; "
+                        "latency from scheduled arrival to solution in host memory",
+            "rates_req_s": SERVE_RATES, "modes": out}
 
 
 def cpu_reference_sample(steps: int, warmup: int, n: int = 128):
@@ -395,21 +574,30 @@ def run_ours(args):
         a[...] = f.cpu().numpy()
         h_rhs.append(a)
     del rhs_dev
-    h_out = pinned_empty((n, n, n), np.complex128)
+    # one stream and one page-locked output per grid: the four solves are
+    # issued with the asynchronous public calls, so one grid's upload overlaps
+    # another's download and compute
+    h_out = [pinned_empty((n, n, n), np.complex128) for _ in solvers]
+    e2e_streams = [torch.cuda.Stream() for _ in solvers]
+    for M, s in zip(solvers, e2e_streams):
+        M.setStream(s.cuda_stream)
     e2e_steps = max(1, min(args.steps, 3))
-    for M, a in zip(solvers, h_rhs):  # warm-up of the copy path
-        M.assignRhs(a)
-        M.pittPack()
-        M.getSolution(out=h_out)
+
+    def e2e_step():
+        for M, a, o in zip(solvers, h_rhs, h_out):
+            M.assignRhsAsync(a)
+            M.pittPack()
+            M.getSolutionAsync(o)
+        for M in solvers:
+            M.synchronize()
+
+    e2e_step()  # warm-up of the copy path
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     w0 = time.perf_counter()
     for _ in range(e2e_steps):
-        for M, a in zip(solvers, h_rhs):
-            M.assignRhs(a)
-            M.pittPack()
-            M.getSolution(out=h_out)
+        e2e_step()
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - w0
     if dist:
@@ -417,6 +605,16 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e_val = world * e2e_steps * len(FAMILIES) * npts / e2e_s / 1e6
+
+    for M in solvers:
+        M.close()
+    del h_rhs, h_out, ref_buf, mix_buf
+    torch.cuda.empty_cache()
+    batch = serve = None
+    if world == 1 and not args.no_batch:
+        batch = run_batch_leg(args, torch, stream)
+    if world == 1 and not args.no_serve:
+        serve = run_serve_leg(args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -444,10 +642,10 @@ def run_ours(args):
             "gpu_launches": results[best]["gpu_launches"],
             "clocks": clk,
             "cpu_baseline": cpu,
+            "batch": batch,
+            "serving": serve,
         }
         print(json.dumps(line), flush=True)
-    for M in solvers:
-        M.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -463,6 +661,9 @@ def main():
     ap.add_argument("--n", type=int, default=N_GRID, help="grid edge (the benchmark uses 512)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--sweeps", type=int, default=1, help="refinement sweeps of the mixed-precision mode")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 96-grid batched workload")
+    ap.add_argument("--no-serve", action="store_true", help="skip the request-stream workload")
+    ap.add_argument("--serve-requests", type=int, default=160, help="requests per arrival rate")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
