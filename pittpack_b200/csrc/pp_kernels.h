@@ -47,6 +47,7 @@ struct PPLinePassArgs {
     const void* tw;    // FFT twiddles (double2 or float2), length n or n/2
     const void* cs2;   // family twiddles in the kernel's precision
     int in_cplx, out_cplx;
+    int vec16;          // power-of-two kernel: src and its run starts are 16-byte aligned
     // refinement epilogue of the inverse x pass (acc != null): the real part v
     // of each output becomes u = acc + out_scale v + zplane[plane] in FP64;
     // written to acc, or (dst != null) as the final complex-interleaved P

@@ -1,0 +1,459 @@
+// Transform pass for power-of-two line lengths: the same four passes and the
+// same per-family pre/post-processing as pp_linepass.cu (see the reference
+// citations there), built on the register-resident FFT of pp_fftreg.cuh and
+// specialised at compile time on the boundary family, so that reorders,
+// signs and twiddle selection cost no run-time branches.
+//
+//   FFT family (P-P): LPC complex lines per CTA, one FFT of N each.
+//   DCT-II/III, DST-II/III (N-N, D-D): 2 LPC real lines per CTA, packed two
+//     to a complex FFT of N (z = v1 + i v2) and separated exactly afterwards:
+//     V1_k = (Z_k + conj Z_{N-k}) / 2, V2_k = (Z_k - conj Z_{N-k}) / (2i);
+//     inverse: Z = V1 + i V2 of two Hermitian spectra, z = v1 + i v2.
+//   DCT-IV, DST-IV (N-D, D-N): 2 LPC real lines per CTA, one complex FFT of
+//     N/2 each.
+//
+// Phases: (1) the raw tile is copied into shared memory by cp.async, 16-byte
+// chunks where the layout allows (a line of N elements, or for the strided y
+// pass a row segment of the tile's lines); (2) each thread gathers its pass-0
+// FFT inputs from the raw tile with the family's reorder folded into the
+// addresses (radix 8 first, so which half a register falls in is known at
+// compile time); (3) FFT; (4) post-processing of pairs (k, N-k), each Z read
+// once, and stores.  The forward x pass's dz^2 scaling is applied to the
+// outputs (a linear factor), the Dirichlet lift is subtracted (divided by
+// dz^2) from the few raw elements on a Dirichlet face.
+#pragma once
+
+#include <type_traits>
+
+#include "pp_common.cuh"
+#include "pp_fftreg.cuh"
+#include "pp_kernels.h"
+
+namespace pp_lp2 {
+
+enum Fam : int { F_DST2 = 0, F_DCT2 = 1, F_FFT = 2, F_Q4 = 3 };
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+    using type = double2;
+};
+template <>
+struct Vec2<float> {
+    using type = float2;
+};
+
+PP_D int mk_pos(int e, int n) { return (e & 1) ? (n - 1 - (e >> 1)) : (e >> 1); }
+
+PP_D double lift_at(const PPLift& L, int i, int j, int k, int nx, int ny, int nz)
+{
+    double s = 0.0;
+    // same order as the reference: z-min, z-max, x-min, x-max, y-min, y-max
+    if (L.z0 && k == 0) s += L.z0[i + (long)nx * j];
+    if (L.z1 && k == nz - 1) s += L.z1[i + (long)nx * j];
+    if (L.x0 && i == 0) s += L.x0[j + (long)ny * k];
+    if (L.x1 && i == nx - 1) s += L.x1[j + (long)ny * k];
+    if (L.y0 && j == 0) s += L.y0[i + (long)nx * k];
+    if (L.y1 && j == ny - 1) s += L.y1[i + (long)nx * k];
+    return s;
+}
+
+// asynchronous global -> shared copy of BYTES (4, 8 or 16)
+template <int BYTES>
+PP_D void cp_async(void* smem, const void* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    if (BYTES == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+    if (BYTES == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+    if (BYTES == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+// shared memory of one CTA: the FFT line buffers (the raw tile aliases them)
+template <typename Real, int N, int LPC>
+constexpr size_t smem_bytes()
+{
+    using C = typename Vec2<Real>::type;
+    constexpr size_t a1 = (size_t)LPC * rp_pitch(N);
+    constexpr size_t a4 = (size_t)2 * LPC * rp_pitch(N / 2);
+    return (a1 > a4 ? a1 : a4) * sizeof(C);
+}
+
+// one output element (line l of the tile, element e): the refinement
+// epilogue (acc set) or a scaled store
+template <typename Real>
+PP_D void put(const PPLinePassArgs& a, long off, int plane, Real re, Real im, Real sc)
+{
+    using C = typename Vec2<Real>::type;
+    if (a.acc) {
+        // u = u_prev + scale * correction + zero-mode constant, in FP64
+        const double u = (a.acc_read ? a.acc[off] : 0.0) + a.out_scale * (double)re +
+                         (a.zplane ? a.zscale * a.zplane[plane] : 0.0);
+        if (a.dst) reinterpret_cast<double2*>(a.dst)[off] = make_double2(u, 0.0);
+        else a.acc[off] = u;
+        return;
+    }
+    if (a.out_cplx) reinterpret_cast<C*>(a.dst)[off] = mkc<C>(sc * re, sc * im);
+    else reinterpret_cast<Real*>(a.dst)[off] = sc * re;
+}
+
+template <typename Real, int N, int LPC, int FAM, bool INVERSE, bool STRIDED>
+__global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
+{
+    using C = typename Vec2<Real>::type;
+    constexpr bool FFTK = FAM == F_FFT;
+    constexpr bool Q4 = FAM == F_Q4;
+    constexpr int NT = LPC * N / 8;
+    constexpr int DL = FFTK ? LPC : 2 * LPC;  // data lines per tile
+    constexpr int LN = rp_log2(N);
+    constexpr int LDL = rp_log2(DL);
+    // raw tile elements: complex for the FFT family, real otherwise
+    using RE = typename std::conditional<FFTK, C, Real>::type;
+    extern __shared__ __align__(16) unsigned char lp2_smem[];
+    C* sb = reinterpret_cast<C*>(lp2_smem);
+    RE* raw = reinterpret_cast<RE*>(lp2_smem);
+
+    const int tid = threadIdx.x;
+    const int tile = blockIdx.x;
+    const int plane = tile / a.tiles_per_plane;
+    const int l0 = (tile - plane * a.tiles_per_plane) * DL;
+    const int nl = min(DL, a.nlines - l0);
+    const long base = (long)plane * a.plane_stride + (long)l0 * a.line_stride;
+    const C* tw = reinterpret_cast<const C*>(a.tw);
+    const C* cs = reinterpret_cast<const C*>(a.cs2);
+    // raw position of (line l, element e)
+    auto ridx = [](int l, int e) -> int { return STRIDED ? e * DL + l : l * N + e; };
+
+    // ---- 1. load the raw tile ----------------------------------------------------------
+    // full tiles whose global element type equals the raw one go in 16-byte
+    // chunks (a line of N elements, or a row segment of DL elements); the
+    // rest element by element (real <-> complex conversion, partial tiles)
+    const bool same = FFTK ? (a.in_cplx != 0) : (a.in_cplx == 0);
+    constexpr int RUN = STRIDED ? DL : N;            // elements per contiguous run
+    constexpr int PER = 16 / (int)sizeof(RE);        // elements per 16-byte chunk
+    constexpr bool VOK = (RUN * (int)sizeof(RE)) % 16 == 0;  // runs are whole chunks
+    if (VOK && same && a.vec16 && nl == DL) {
+        constexpr int CPR = VOK ? RUN / PER : 1;     // chunks per run
+        constexpr int TOT = (STRIDED ? N : DL) * CPR;
+        const RE* src = reinterpret_cast<const RE*>(a.src);
+        for (int c = tid; c < TOT; c += NT) {
+            const int r = c / CPR;  // run: element row (strided) or line
+            const int k = (c - r * CPR) * PER;
+            const long goff = base + (STRIDED ? (long)r * a.elem_stride : (long)r * a.line_stride) + k;
+            cp_async<16>(raw + r * RUN + k, src + goff);
+        }
+    } else {
+        for (int idx = tid; idx < DL * N; idx += NT) {
+            int l, e;
+            if (STRIDED) {
+                l = idx & (DL - 1);
+                e = idx >> LDL;
+            } else {
+                l = idx >> LN;
+                e = idx & (N - 1);
+            }
+            Real* d = reinterpret_cast<Real*>(raw + ridx(l, e));
+            if (l < nl) {
+                const long off = base + (long)l * a.line_stride + (long)e * a.elem_stride;
+                const Real* s = reinterpret_cast<const Real*>(a.src);
+                if (FFTK) {
+                    if (a.in_cplx) {
+                        cp_async<2 * sizeof(Real)>(d, s + 2 * off);
+                    } else {
+                        cp_async<sizeof(Real)>(d, s + off);
+                        d[1] = (Real)0;
+                    }
+                } else {
+                    // the DCT/DST families read the real part only
+                    cp_async<sizeof(Real)>(d, s + (a.in_cplx ? 2 * off : off));
+                }
+            } else {
+                d[0] = (Real)0;
+                if (FFTK) d[1] = (Real)0;
+            }
+        }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+
+    // ---- 1b. Dirichlet lift (forward x pass of the plain solve) ---------------------
+    // b = f dz^2 - lift; the dz^2 factor is applied to the outputs, so the
+    // raw elements on a Dirichlet face lose lift / dz^2 here
+    if (a.rhs_scale && a.lift.any) {
+        const double inv = 1.0 / (a.dz * a.dz);
+        const PPLift& L = a.lift;
+        const bool whole = (L.z0 && plane == 0) || (L.z1 && plane == a.nz - 1) || (L.y0 && l0 == 0) ||
+                           (L.y1 && l0 + nl >= a.ny);
+        if (whole) {
+            for (int idx = tid; idx < nl * N; idx += NT) {
+                const int l = idx >> LN, e = idx & (N - 1);
+                Real* d = reinterpret_cast<Real*>(raw + ridx(l, e));
+                d[0] = d[0] - (Real)(lift_at(L, e, l0 + l, plane, a.nx, a.ny, a.nz) * inv);
+            }
+        } else if (L.x0 || L.x1) {
+            for (int idx = tid; idx < 2 * nl; idx += NT) {
+                const int l = idx >> 1, e = (idx & 1) ? N - 1 : 0;
+                Real* d = reinterpret_cast<Real*>(raw + ridx(l, e));
+                d[0] = d[0] - (Real)(lift_at(L, e, l0 + l, plane, a.nx, a.ny, a.nz) * inv);
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- 2. pass-0 registers: the family's pre-processing, from the raw tile ----------
+    // radix 8 first: register q holds point m = t + q N/8 (t < N/8), so the
+    // half of the line it falls in is known from q at compile time
+    constexpr int NF = Q4 ? N / 2 : N;  // FFT length
+    constexpr int TPL = NF / 8;         // threads per FFT line
+    static_assert(rp_radix(NF, 0) == 8, "the first pass is radix 8");
+    const int fl = tid / TPL;           // FFT line of this thread
+    const int t = tid - fl * TPL;
+    C* line = sb + fl * (Q4 ? rp_pitch(N / 2) : rp_pitch(N));
+    C v[8];
+    if constexpr (FFTK) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = raw[ridx(fl, t + q * (N / 8))];
+    } else if constexpr (Q4) {
+        // z_m = (x[2m] + i x[N-1-2m]) e^{-i pi m / N}; DST-IV reverses its input
+        const bool rev = a.kind == PP_KIND_DST4;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int m = t + q * (NF / 8);
+            const int ea = 2 * m, eb = N - 1 - 2 * m;
+            const Real xa = raw[ridx(fl, rev ? N - 1 - ea : ea)];
+            const Real xb = raw[ridx(fl, rev ? N - 1 - eb : eb)];
+            const C w = __ldg(&cs[m]);
+            v[q] = mkc<C>(xa * w.x - xb * w.y, xa * w.y + xb * w.x);
+        }
+    } else if constexpr (!INVERSE) {
+        // DCT-II: Makhoul reorder v[m] = x[2m] (m < N/2), x[2N-1-2m] (m >= N/2);
+        // DST-II first swaps x'[j] = (-1)^j x[N-1-j]: v[m] = x[N-1-2m] or -x[2m-N]
+        const int la = 2 * fl, lb = la + 1;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int m = t + q * (N / 8);
+            int e;
+            if (FAM == F_DCT2) e = q < 4 ? 2 * m : 2 * N - 1 - 2 * m;
+            else e = q < 4 ? N - 1 - 2 * m : 2 * m - N;
+            const Real s = (FAM == F_DST2 && q >= 4) ? (Real)-1 : (Real)1;
+            v[q] = mkc<C>(s * raw[ridx(la, e)], s * raw[ridx(lb, e)]);
+        }
+    } else {
+        // DCT-III pre-processing of both packed spectra; Z = V1 + i V2.  DST-III
+        // reads the reversed line and carries (-1)^m
+        const int la = 2 * fl, lb = la + 1;
+        auto X = [&](int k) -> C {
+            const int e = FAM == F_DCT2 ? k : N - 1 - k;
+            return mkc<C>(raw[ridx(la, e)], raw[ridx(lb, e)]);
+        };
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int m = t + q * (N / 8);
+            const C Xm = X(m);
+            C V1, V2;
+            if (q == 0 && t == 0) {
+                V1 = mkc<C>((Real)0.5 * Xm.x, 0);
+                V2 = mkc<C>((Real)0.5 * Xm.y, 0);
+            } else {
+                const C Xn = X(N - m);
+                if (q < 4 || (q == 4 && t == 0)) {
+                    const C w = __ldg(&cs[m]);
+                    V1 = mkc<C>((Real)0.5 * (w.x * Xm.x + w.y * Xn.x), (Real)0.5 * (w.y * Xm.x - w.x * Xn.x));
+                    V2 = mkc<C>((Real)0.5 * (w.x * Xm.y + w.y * Xn.y), (Real)0.5 * (w.y * Xm.y - w.x * Xn.y));
+                } else {
+                    const C w = __ldg(&cs[N - m]);
+                    V1 = mkc<C>((Real)0.5 * (w.x * Xn.x + w.y * Xm.x), -((Real)0.5 * (w.y * Xn.x - w.x * Xm.x)));
+                    V2 = mkc<C>((Real)0.5 * (w.x * Xn.y + w.y * Xm.y), -((Real)0.5 * (w.y * Xn.y - w.x * Xm.y)));
+                }
+            }
+            C Z = mkc<C>(V1.x - V2.y, V1.y + V2.x);
+            if (FAM == F_DST2 && (t & 1)) Z = mkc<C>(-Z.x, -Z.y);  // m and t have the same parity
+            v[q] = Z;
+        }
+    }
+
+    // ---- 3. FFT (its first exchange starts with a barrier, so the raw tile
+    //         that aliases the line buffers is no longer needed) ----------------------
+    if (INVERSE && !Q4) rp_fft<+1, NF>(v, line, t, tw);
+    else rp_fft<-1, NF>(v, line, t, tw);
+    __syncthreads();  // all reads of the last exchange are done
+#pragma unroll
+    for (int j = 0; j < 8; ++j) line[rp_pad(rp_out_index<NF>(t, j))] = v[j];
+    __syncthreads();
+
+    // ---- 4. post-processing and stores ------------------------------------------------
+    // thread -> (line, index): the strided pass runs the line fastest, so that
+    // a warp writes row segments; the contiguous pass runs the index fastest
+    const Real sc = (Real)(a.out_scale * (a.rhs_scale ? a.dz * a.dz : 1.0));
+    auto goff = [&](int l, int e) -> long { return base + (long)l * a.line_stride + (long)e * a.elem_stride; };
+    constexpr int P1 = rp_pitch(N);
+    if constexpr (FFTK) {
+        for (int idx = tid; idx < LPC * N; idx += NT) {
+            int l, e;
+            if (STRIDED) {
+                l = idx & (LPC - 1);
+                e = idx >> rp_log2(LPC);
+            } else {
+                l = idx >> LN;
+                e = idx & (N - 1);
+            }
+            if (l >= nl) continue;
+            const C z = sb[l * P1 + rp_pad(e)];
+            put<Real>(a, goff(l, e), plane, z.x, z.y, sc);
+        }
+    } else if constexpr (Q4) {
+        // w_p = e^{-i pi (4p+1)/(4N)} Z_p: X[2p] = c Re w_p, X[N-1-2p] = -c Im w_p
+        // (c = 2 forward, 1 inverse); DST-IV flips the sign of the odd outputs
+        constexpr int NH = N / 2, P4 = rp_pitch(N / 2);
+        const Real c = INVERSE ? (Real)1 : (Real)2;
+        const Real so = a.kind == PP_KIND_DST4 ? c : -c;
+        for (int idx = tid; idx < DL * NH; idx += NT) {
+            int l, p;
+            if (STRIDED) {
+                l = idx & (DL - 1);
+                p = idx >> LDL;
+            } else {
+                l = idx >> (LN - 1);
+                p = idx & (NH - 1);
+            }
+            if (l >= nl) continue;
+            const C z = sb[l * P4 + rp_pad(p)];
+            const C w = __ldg(&cs[NH + p]);
+            const Real wr = z.x * w.x - z.y * w.y;
+            const Real wi = z.x * w.y + z.y * w.x;
+            put<Real>(a, goff(l, 2 * p), plane, c * wr, (Real)0, sc);
+            put<Real>(a, goff(l, N - 1 - 2 * p), plane, so * wi, (Real)0, sc);
+        }
+    } else if constexpr (!INVERSE) {
+        // pairs (k, N-k) of both packed lines: X_k = 2 (Re V_k cos t_k + Im V_k sin t_k),
+        // output e = k (DCT-II) or e = N-1-k with sign (-1)^e (DST-II)
+        constexpr int LL = rp_log2(LPC);
+        for (int idx = tid; idx < LPC * (N / 2); idx += NT) {
+            int cl, kk;
+            if (STRIDED) {
+                cl = idx & (LPC - 1);
+                kk = idx >> LL;
+            } else {
+                cl = idx >> (LN - 1);
+                kk = idx & (N / 2 - 1);
+            }
+            const int la = 2 * cl, lb = la + 1;
+            const C* ln = sb + cl * P1;
+            const int k1 = kk == 0 ? 0 : kk;
+            const int k2 = kk == 0 ? N / 2 : N - kk;
+            const C Z1 = ln[rp_pad(k1)];
+            const C Z2 = ln[rp_pad(k2)];
+            // partners: Z_{N-k1} = Z2 and Z_{N-k2} = Z1, except at k = 0 and N/2
+            const C P1z = kk == 0 ? Z1 : Z2;
+            const C P2z = kk == 0 ? Z2 : Z1;
+            const C w1 = __ldg(&cs[k1]);
+            const C w2 = __ldg(&cs[k2]);
+            auto emit = [&](int k, C Zk, C Zn, C w) {
+                // V1 (line a) and V2 (line b) at k
+                const Real v1x = (Real)0.5 * (Zk.x + Zn.x), v1y = (Real)0.5 * (Zk.y - Zn.y);
+                const Real v2x = (Real)0.5 * (Zk.y + Zn.y), v2y = -(Real)0.5 * (Zk.x - Zn.x);
+                int e = k;
+                Real sg = (Real)2;
+                if (FAM == F_DST2) {
+                    e = N - 1 - k;
+                    if (e & 1) sg = (Real)-2;
+                }
+                if (la < nl) put<Real>(a, goff(la, e), plane, sg * (v1x * w.x + v1y * w.y), (Real)0, sc);
+                if (lb < nl) put<Real>(a, goff(lb, e), plane, sg * (v2x * w.x + v2y * w.y), (Real)0, sc);
+            };
+            emit(k1, Z1, P1z, w1);
+            emit(k2, Z2, P2z, w2);
+        }
+    } else {
+        // DCT-III output reorder x[2i] = Re v[i], x[2i+1] = Re v[N-1-i] of both
+        // packed lines; DST-III reverses with sign (-1)^e
+        constexpr int LL = rp_log2(LPC);
+        for (int idx = tid; idx < LPC * N; idx += NT) {
+            int cl, e;
+            if (STRIDED) {
+                cl = idx & (LPC - 1);
+                e = idx >> LL;
+            } else {
+                cl = idx >> LN;
+                e = idx & (N - 1);
+            }
+            const int la = 2 * cl, lb = la + 1;
+            int j = e;
+            Real sg = (Real)1;
+            if (FAM == F_DST2) {
+                j = N - 1 - e;
+                if (e & 1) sg = (Real)-1;
+            }
+            const C z = sb[cl * P1 + rp_pad(mk_pos(j, N))];
+            if (la < nl) put<Real>(a, goff(la, e), plane, sg * z.x, (Real)0, sc);
+            if (lb < nl) put<Real>(a, goff(lb, e), plane, sg * z.y, (Real)0, sc);
+        }
+    }
+}
+
+template <typename Real, int N, int LPC, int FAM>
+cudaError_t launch_fam(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
+{
+    constexpr size_t smem = smem_bytes<Real, N, LPC>();
+    dim3 grid(a.nplanes * a.tiles_per_plane), block(LPC * N / 8);
+#define PP_LP2(INV, STR)                                                                                    \
+    do {                                                                                                    \
+        auto kfn = lp2_kernel<Real, N, LPC, FAM, INV, STR>;                                                      \
+        cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        if (e != cudaSuccess) return e;                                                                     \
+        kfn<<<grid, block, smem, st>>>(a);                                                                  \
+        return cudaGetLastError();                                                                          \
+    } while (0)
+    if (inverse && strided) PP_LP2(true, true);
+    if (inverse && !strided) PP_LP2(true, false);
+    if (!inverse && strided) PP_LP2(false, true);
+    PP_LP2(false, false);
+#undef PP_LP2
+}
+
+template <typename Real, int N, int LPC>
+cudaError_t launch_n(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
+{
+    switch (a.kind) {
+    case PP_KIND_DST2: return launch_fam<Real, N, LPC, F_DST2>(a, inverse, strided, st);
+    case PP_KIND_DCT2: return launch_fam<Real, N, LPC, F_DCT2>(a, inverse, strided, st);
+    case PP_KIND_FFT: return launch_fam<Real, N, LPC, F_FFT>(a, inverse, strided, st);
+    default: return launch_fam<Real, N, LPC, F_Q4>(a, inverse, strided, st);
+    }
+}
+
+// lines per CTA (complex FFT lines) for a power-of-two length; 0 if the
+// length has no specialised kernel
+inline int lpc_of(int n)
+{
+    switch (n) {
+    case 16: return 16;
+    case 32: return 16;
+    case 64: return 8;
+    case 128: return 8;
+    case 256: return 4;
+    case 512: return 4;
+    case 1024: return 2;
+    case 2048: return 1;
+    default: return 0;
+    }
+}
+
+template <typename Real>
+cudaError_t launch(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
+{
+    switch (a.n) {
+    case 16: return launch_n<Real, 16, 16>(a, inverse, strided, st);
+    case 32: return launch_n<Real, 32, 16>(a, inverse, strided, st);
+    case 64: return launch_n<Real, 64, 8>(a, inverse, strided, st);
+    case 128: return launch_n<Real, 128, 8>(a, inverse, strided, st);
+    case 256: return launch_n<Real, 256, 4>(a, inverse, strided, st);
+    case 512: return launch_n<Real, 512, 4>(a, inverse, strided, st);
+    case 1024: return launch_n<Real, 1024, 2>(a, inverse, strided, st);
+    case 2048: return launch_n<Real, 2048, 1>(a, inverse, strided, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace pp_lp2

@@ -353,6 +353,16 @@ int pick_lines_fp32(int nfft)
     return L;
 }
 
+// whether every contiguous run of a transform tile starts on a 16-byte
+// boundary: the source pointer and the plane / line (contiguous pass) or
+// element (strided pass) strides, in bytes
+int runs_aligned16(const PPLinePassArgs& a, bool strided, size_t elem_bytes)
+{
+    if (reinterpret_cast<uintptr_t>(a.src) % 16) return 0;
+    const size_t st = strided ? (size_t)a.elem_stride : (size_t)a.line_stride;
+    return ((size_t)a.plane_stride * elem_bytes) % 16 == 0 && (st * elem_bytes) % 16 == 0;
+}
+
 // one transform pass: the register-resident kernel for power-of-two lengths,
 // the generic shared-memory Stockham kernel otherwise
 cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool strided, bool in_cplx,
@@ -372,6 +382,7 @@ cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool s
         a.cs2 = d.csf.p;
         a.in_cplx = in_cplx;
         a.out_cplx = out_cplx;
+        a.vec16 = runs_aligned16(a, strided, (in_cplx ? 2 : 1) * sizeof(float));
         const int dl = d.kind == PP_KIND_FFT ? lpc : 2 * lpc;
         a.L = dl;
         a.tiles_per_plane = (a.nlines + dl - 1) / dl;
@@ -382,6 +393,7 @@ cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool s
         a.cs2 = d.cs.p;
         a.in_cplx = in_cplx;
         a.out_cplx = out_cplx;
+        a.vec16 = runs_aligned16(a, strided, (in_cplx ? 2 : 1) * sizeof(double));
         const int dl = d.kind == PP_KIND_FFT ? lpc : 2 * lpc;
         a.L = dl;
         a.tiles_per_plane = (a.nlines + dl - 1) / dl;
