@@ -69,14 +69,31 @@ PP_D void cp_async(void* smem, const void* gmem)
     if (BYTES == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 
-// shared memory of one CTA: the FFT line buffers (the raw tile aliases them)
-template <typename Real, int N, int LPC>
+// row pitch (elements) of the strided pass's raw tile [element][line]: the
+// smallest pitch above the tile's line count whose rows start on 16-byte
+// boundaries and are an odd number of 16-byte units apart, so that threads
+// reading consecutive rows fall in different banks
+template <int FAM, int LPC>
+constexpr int raw_row_pitch(int elem_bytes)
+{
+    const int dl = FAM == F_FFT ? LPC : 2 * LPC;
+    int rp = dl + 1;
+    while ((rp * elem_bytes) % 16 != 0 || ((rp * elem_bytes / 16) & 1) == 0) ++rp;
+    return rp;
+}
+
+// shared memory of one CTA: the FFT line buffers, or the raw tile that
+// aliases them if that is larger (the padded strided tile)
+template <typename Real, int N, int LPC, int FAM, bool STRIDED>
 constexpr size_t smem_bytes()
 {
     using C = typename Vec2<Real>::type;
-    constexpr size_t a1 = (size_t)LPC * rp_pitch(N);
-    constexpr size_t a4 = (size_t)2 * LPC * rp_pitch(N / 2);
-    return (a1 > a4 ? a1 : a4) * sizeof(C);
+    constexpr size_t a1 = (size_t)LPC * rp_pitch(N) * sizeof(C);
+    constexpr size_t a4 = (size_t)2 * LPC * rp_pitch(N / 2) * sizeof(C);
+    constexpr size_t lines = a1 > a4 ? a1 : a4;
+    constexpr size_t re = FAM == F_FFT ? sizeof(C) : sizeof(Real);
+    constexpr size_t raw = (size_t)N * (STRIDED ? raw_row_pitch<FAM, LPC>((int)re) : (FAM == F_FFT ? LPC : 2 * LPC)) * re;
+    return lines > raw ? lines : raw;
 }
 
 // one output element (line l of the tile, element e): the refinement
@@ -122,7 +139,8 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     const C* tw = reinterpret_cast<const C*>(a.tw);
     const C* cs = reinterpret_cast<const C*>(a.cs2);
     // raw position of (line l, element e)
-    auto ridx = [](int l, int e) -> int { return STRIDED ? e * DL + l : l * N + e; };
+    constexpr int RP = raw_row_pitch<FAM, LPC>((int)sizeof(RE));
+    auto ridx = [](int l, int e) -> int { return STRIDED ? e * RP + l : l * N + e; };
 
     // ---- 1. load the raw tile ----------------------------------------------------------
     // full tiles whose global element type equals the raw one go in 16-byte
@@ -140,7 +158,7 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
             const int r = c / CPR;  // run: element row (strided) or line
             const int k = (c - r * CPR) * PER;
             const long goff = base + (STRIDED ? (long)r * a.elem_stride : (long)r * a.line_stride) + k;
-            cp_async<16>(raw + r * RUN + k, src + goff);
+            cp_async<16>(raw + r * (STRIDED ? RP : N) + k, src + goff);
         }
     } else {
         for (int idx = tid; idx < DL * N; idx += NT) {
@@ -237,7 +255,13 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
             if (FAM == F_DCT2) e = q < 4 ? 2 * m : 2 * N - 1 - 2 * m;
             else e = q < 4 ? N - 1 - 2 * m : 2 * m - N;
             const Real s = (FAM == F_DST2 && q >= 4) ? (Real)-1 : (Real)1;
-            v[q] = mkc<C>(s * raw[ridx(la, e)], s * raw[ridx(lb, e)]);
+            if (STRIDED) {
+                // lines la, lb are adjacent in a row: one 16-byte read
+                const C z = *reinterpret_cast<const C*>(raw + ridx(la, e));
+                v[q] = mkc<C>(s * z.x, s * z.y);
+            } else {
+                v[q] = mkc<C>(s * raw[ridx(la, e)], s * raw[ridx(lb, e)]);
+            }
         }
     } else {
         // DCT-III pre-processing of both packed spectra; Z = V1 + i V2.  DST-III
@@ -245,6 +269,7 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
         const int la = 2 * fl, lb = la + 1;
         auto X = [&](int k) -> C {
             const int e = FAM == F_DCT2 ? k : N - 1 - k;
+            if (STRIDED) return *reinterpret_cast<const C*>(raw + ridx(la, e));
             return mkc<C>(raw[ridx(la, e)], raw[ridx(lb, e)]);
         };
 #pragma unroll
@@ -395,10 +420,10 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
 template <typename Real, int N, int LPC, int FAM>
 cudaError_t launch_fam(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
 {
-    constexpr size_t smem = smem_bytes<Real, N, LPC>();
     dim3 grid(a.nplanes * a.tiles_per_plane), block(LPC * N / 8);
 #define PP_LP2(INV, STR)                                                                                    \
     do {                                                                                                    \
+        constexpr size_t smem = smem_bytes<Real, N, LPC, FAM, STR>();                                       \
         auto kfn = lp2_kernel<Real, N, LPC, FAM, INV, STR>;                                                      \
         cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
         if (e != cudaSuccess) return e;                                                                     \
