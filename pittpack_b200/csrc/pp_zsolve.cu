@@ -62,6 +62,11 @@ PP_D void cp_async16(void* smem, const void* gmem)
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+PP_D void cp_async4(void* smem, const void* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
 PP_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // skewed position of row k inside a system's column of the tile
@@ -74,10 +79,12 @@ struct ZLayout {
     int mmax;        // table rows per group
     int groups;      // groups (systems in flight) per CTA
     int P;           // lanes per system
-    size_t tile_off, tab_off, red_off, bytes;
+    size_t tile_off, tab_off, red_off, stg_off, bytes;
 };
 
-PP_HD ZLayout zlayout(int TS, int nz, int P, bool cplx, int nthreads)
+// g32: the FP32 spectrum is first copied into a staging area [k][s] of
+// TS x nz FP32 elements behind the rest
+PP_HD ZLayout zlayout(int TS, int nz, int P, bool cplx, int nthreads, bool g32 = false)
 {
     ZLayout L;
     const size_t e = cplx ? 16 : 8;
@@ -89,8 +96,13 @@ PP_HD ZLayout zlayout(int TS, int nz, int P, bool cplx, int nthreads)
     L.tab_off = (size_t)TS * L.pitch * e;
     L.tab_off = (L.tab_off + 15) & ~(size_t)15;
     L.red_off = L.tab_off + (size_t)TS * L.mmax * 16;
-    // per group: 2P rows of a, c, u (doubles) and d (element)
-    L.bytes = L.red_off + (size_t)L.groups * 2 * P * (24 + e);
+    // per group: 2P rows of a, c, u (doubles) and d (element); before the
+    // sweeps the same bytes hold the b_i recurrence of every system (TS x mmax)
+    const size_t red = (size_t)L.groups * 2 * P * (24 + e);
+    const size_t scr = (size_t)TS * L.mmax * 8;
+    L.bytes = L.red_off + (red > scr ? red : scr);
+    L.stg_off = (L.bytes + 15) & ~(size_t)15;
+    if (g32) L.bytes = L.stg_off + (size_t)TS * nz * (cplx ? 8 : 4);
     return L;
 }
 
@@ -110,8 +122,11 @@ struct ZTo32<double2> {
 };
 
 // G32: the spectrum in global memory is FP32 (refined mixed-precision solve);
-// the tile and all arithmetic stay FP64
-template <bool CPLX, bool G32>
+// the tile and all arithmetic stay FP64.  MT > 0: every lane owns exactly MT
+// rows (nz = P MT) and keeps them in registers through the three sweeps,
+// reading and writing its rows of the tile once; MT = 0: any nz, the sweeps
+// work on the tile in shared memory.
+template <bool CPLX, bool G32, int MT>
 __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
 {
     using T = typename std::conditional<CPLX, double2, double>::type;
@@ -119,7 +134,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     extern __shared__ __align__(16) unsigned char zsm_raw[];
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int P = a.P;
-    const ZLayout Lz = zlayout(a.TS, nz, P, CPLX, blockDim.x);
+    const ZLayout Lz = zlayout(a.TS, nz, P, CPLX, blockDim.x, G32);
     T* tile = reinterpret_cast<T*>(zsm_raw + Lz.tile_off);
 
     const int group = threadIdx.x / P;
@@ -147,20 +162,12 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         const int kstep = blockDim.x >> lts;
         if (s < ts) {
             if (G32) {
-                // converting loads, 8 in flight per thread
-                constexpr int ZU = 8;
-                for (int k0 = threadIdx.x >> lts; k0 < nz; k0 += ZU * kstep) {
-                    T32 v[ZU];
-#pragma unroll
-                    for (int u = 0; u < ZU; ++u) {
-                        const int k = k0 + u * kstep;
-                        if (k < nz) v[u] = g32[k * plane + col0 + s];
-                    }
-#pragma unroll
-                    for (int u = 0; u < ZU; ++u) {
-                        const int k = k0 + u * kstep;
-                        if (k < nz) tile[s * Lz.pitch + zpos(k)] = ZTo32<T>::up(v[u]);
-                    }
+                // FP32 elements copied asynchronously into the staging area;
+                // converted to the FP64 tile once they have landed
+                T32* stg = reinterpret_cast<T32*>(zsm_raw + Lz.stg_off);
+                for (int k = threadIdx.x >> lts; k < nz; k += kstep) {
+                    if (sizeof(T32) == 8) cp_async8(&stg[k * a.TS + s], &g32[k * plane + col0 + s]);
+                    else cp_async4(&stg[k * a.TS + s], &g32[k * plane + col0 + s]);
                 }
             } else {
                 for (int k = threadIdx.x >> lts; k < nz; k += kstep)
@@ -177,20 +184,25 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     // One thread per system; the divisions are independent.  |b_i| grows like
     // |lambda|^i, so where mm log2|lambda| could leave the double range the
     // division recurrence is used instead.
+    // Phase 1, one thread per system: b_i by the recurrence (FMAs only) into
+    // the scratch bytes, or -- where |b_i| could overflow -- the division
+    // recurrence straight into the table, marked by b_0 = 0.
+    double* bsc = reinterpret_cast<double*>(zsm_raw + Lz.red_off);
+    const int mm = Lz.mmax;
     for (int s = threadIdx.x; s < ts; s += blockDim.x) {
         const double lam = (-2.0 + a.ax[kx0 + s] * a.Cx) + a.ay[ky] * a.Cy;
-        double2* tb = reinterpret_cast<double2*>(zsm_raw + Lz.tab_off) + (size_t)s * Lz.mmax;
-        const int mm = Lz.mmax;
+        double* b = bsc + (size_t)s * mm;
         if ((double)mm * log2(fabs(lam) + 1.0) < 900.0) {
-            double bm = 1.0, bc = lam, sg = 1.0;
+            double bm = 1.0, bc = lam;
+            b[0] = 1.0;
             for (int i = 1; i < mm; ++i) {
-                tb[i] = make_double2(bm / bc, sg / bc);
+                b[i] = bc;
                 const double bn = lam * bc - bm;
                 bm = bc;
                 bc = bn;
-                sg = -sg;
             }
         } else {
+            double2* tb = reinterpret_cast<double2*>(zsm_raw + Lz.tab_off) + (size_t)s * mm;
             double gp = 0.0, ap = 0.0;
             for (int i = 1; i < mm; ++i) {
                 const double p = (i == 1) ? 1.0 / lam : 1.0 / (lam - gp);
@@ -199,14 +211,35 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
                 gp = p;
                 ap = al;
             }
+            b[0] = 0.0;
         }
+    }
+    __syncthreads();
+    // Phase 2, every thread: gamma_i = b_{i-1} / b_i, alpha_i = (-1)^{i-1} / b_i,
+    // one reciprocal per entry, the entries of all systems spread over the CTA
+    for (int idx = threadIdx.x; idx < ts * mm; idx += blockDim.x) {
+        const int s = idx / mm, i = idx - s * mm;
+        const double* b = bsc + (size_t)s * mm;
+        if (i == 0 || b[0] == 0.0) continue;
+        const double inv = 1.0 / b[i];
+        reinterpret_cast<double2*>(zsm_raw + Lz.tab_off)[(size_t)s * mm + i] =
+            make_double2(b[i - 1] * inv, (i & 1) ? inv : -inv);
     }
     cp_async_wait_all();
     __syncthreads();
+    if (G32) {
+        const T32* stg = reinterpret_cast<const T32*>(zsm_raw + Lz.stg_off);
+        const int s = threadIdx.x & (a.TS - 1);
+        const int kstep = blockDim.x >> lts;
+        if (s < ts)
+            for (int k = threadIdx.x >> lts; k < nz; k += kstep)
+                tile[s * Lz.pitch + zpos(k)] = ZTo32<T>::up(stg[k * a.TS + s]);
+        __syncthreads();
+    }
 
     const int bsz = nz / P;
     const int rem = nz - bsz * P;
-    const int M = bsz + (lane < rem ? 1 : 0);
+    const int M = MT > 0 ? MT : bsz + (lane < rem ? 1 : 0);
     const int s0 = lane * bsz + min(lane, rem);
     const bool periodic = a.zlo == PP_Z_PERIODIC;
     const bool has_d = a.zlo == PP_Z_DIRICHLET || a.zhi == PP_Z_DIRICHLET;
@@ -224,6 +257,16 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         const bool pin = zero && (periodic || a.pin_always || !has_d);
         T* col = tile + (live ? s : 0) * Lz.pitch;
         const double2* tab = reinterpret_cast<const double2*>(zsm_raw + Lz.tab_off) + (size_t)(live ? s : 0) * Lz.mmax;
+        // the lane's rows: registers (MT > 0) or the tile column
+        T xr[MT > 0 ? MT : 1];
+        if constexpr (MT > 0) {
+#pragma unroll
+            for (int i = 0; i < MT; ++i) xr[i] = live ? col[zpos(s0 + i)] : zzero<T>();
+        }
+        auto X = [&](int i) -> T& {
+            if constexpr (MT > 0) return xr[i];
+            else return col[zpos(s0 + i)];
+        };
 
         double A0, B0, C0, AN, BN, CN;
         if (periodic) {
@@ -254,11 +297,14 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         T rD0 = zzero<T>(), dprev = zzero<T>();
         double aprev = 0.0, gprev = 0.0;
         if (live) {
-            rD0 = col[zpos(s0)];
+            rD0 = X(0);
+            // the tile still holds every lane's input here (registers are
+            // written back at the end)
             if (s0 == 0 && periodic && pin) rD0 = zmul(0.5, zadd(rD0, col[zpos(nz - 1)]));
+#pragma unroll
             for (int i = 1; i < M; ++i) {
                 const int gk = s0 + i;
-                const T D = col[zpos(gk)];
+                const T D = X(i);
                 double al, ga;
                 T dn;
                 if (gk != nz - 1) {
@@ -277,7 +323,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
                     ga = CN * p;
                     dn = zmul(p, zsub(D, zmul(AN, dprev)));
                 }
-                col[zpos(gk)] = dn;
+                X(i) = dn;
                 aprev = al;
                 gprev = ga;
                 dprev = dn;
@@ -295,10 +341,11 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             const double2 t2 = tab[M - 2];
             br = t2.y;
             cr = t2.x;
-            dr = col[zpos(s0 + M - 2)];
+            dr = X(M - 2);
+#pragma unroll
             for (int i = M - 3; i >= 1; --i) {
                 const double2 ti = tab[i];
-                dr = zsub(col[zpos(s0 + i)], zmul(ti.x, dr));
+                dr = zsub(X(i), zmul(ti.x, dr));
                 br = ti.y - ti.x * br;
                 cr = -ti.x * cr;
             }
@@ -402,16 +449,24 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         // ---- recover the block's rows ---------------------------------------------------
         if (live && zero && a.skip_zero) {
             // the kx = ky = 0 column is solved separately (in FP64 from plane sums)
-            for (int i = 0; i < M; ++i) col[zpos(s0 + i)] = zzero<T>();
+#pragma unroll
+            for (int i = 0; i < M; ++i) X(i) = zzero<T>();
         } else if (live) {
             T xn = xl;
-            col[zpos(s0 + M - 1)] = xl;
+            X(M - 1) = xl;
+#pragma unroll
             for (int i = M - 2; i >= 1; --i) {
                 const double2 ti = tab[i];
-                xn = zsub(zsub(col[zpos(s0 + i)], zmul(ti.y, xf)), zmul(ti.x, xn));
-                col[zpos(s0 + i)] = xn;
+                xn = zsub(zsub(X(i), zmul(ti.y, xf)), zmul(ti.x, xn));
+                X(i) = xn;
             }
-            col[zpos(s0)] = xf;
+            X(0) = xf;
+        }
+        if constexpr (MT > 0) {
+            if (live) {
+#pragma unroll
+                for (int i = 0; i < MT; ++i) col[zpos(s0 + i)] = xr[i];
+            }
         }
         __syncwarp(full);
     }
@@ -444,7 +499,7 @@ int pp_zsolve_lanes(int nz, bool cplx)
 }
 
 // launch shape: systems per CTA (one lane group each) and threads per CTA,
-// keeping the CTA within ~112 KB of shared memory so two fit on an SM
+// keeping the CTA within ~56 KB of shared memory so about four fit on an SM
 void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads)
 {
     const int P = pp_zsolve_lanes(nz, cplx);
@@ -453,7 +508,7 @@ void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads)
         const int th = t * P < 32 ? 32 : t * P;
         return zlayout(t, nz, P, cplx, th).bytes;
     };
-    while (ts > 1 && bytes(ts) > 112 * 1024) ts >>= 1;
+    while (ts > 1 && bytes(ts) > 56 * 1024) ts >>= 1;
     while (ts > 1 && ts > nx) ts >>= 1;
     *TS = ts;
     *threads = ts * P < 32 ? 32 : ts * P;
@@ -482,7 +537,7 @@ void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* thre
 {
     const int P = pp_zsolve_valid_lanes(nz, lanes) ? lanes : pp_zsolve_lanes(nz, cplx);
     int ts = PP_Z_THREADS / P;
-    while (ts > 1 && pp_zsolve_smem_p(ts, nz, cplx, P) > 112 * 1024) ts >>= 1;
+    while (ts > 1 && pp_zsolve_smem_p(ts, nz, cplx, P) > 56 * 1024) ts >>= 1;
     while (ts > 1 && ts > nx) ts >>= 1;
     *TS = ts;
     *threads = ts * P < 32 ? 32 : ts * P;
@@ -495,21 +550,32 @@ cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
     if (!pp_zsolve_valid_lanes(a.nz, a.P)) a.P = pp_zsolve_lanes(a.nz, cplx);
     const int threads = a.TS * a.P < 32 ? 32 : a.TS * a.P;
     if (threads > PP_Z_THREADS) return cudaErrorInvalidValue;
-    const size_t smem = pp_zsolve_smem_p(a.TS, a.nz, cplx, a.P);
+    const size_t smem = zlayout(a.TS, a.nz, a.P, cplx, threads, a.data_fp32 != 0).bytes;
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     dim3 grid(a.ny * a.tiles_x), block(threads);
     cudaError_t e;
-#define PP_ZL(C, G)                                                                                             \
+    // rows per lane fixed at compile time where every lane has the same count
+    const int rows = a.nz / a.P;
+    const int mt = (a.nz % a.P == 0 && (rows == 8 || rows == 16 || (rows == 32 && !cplx))) ? rows : 0;
+#define PP_ZL(C, G, M)                                                                                          \
     do {                                                                                                        \
-        auto kfn = zsolve_kernel<C, G>;                                                                         \
+        auto kfn = zsolve_kernel<C, G, M>;                                                                      \
         if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) \
             return e;                                                                                           \
         kfn<<<grid, block, smem, st>>>(a);                                                                      \
     } while (0)
-    if (cplx && a.data_fp32) PP_ZL(true, true);
-    else if (cplx) PP_ZL(true, false);
-    else if (a.data_fp32) PP_ZL(false, true);
-    else PP_ZL(false, false);
+#define PP_ZLM(C, G)                   \
+    do {                               \
+        if (mt == 8) PP_ZL(C, G, 8);   \
+        else if (mt == 16) PP_ZL(C, G, 16); \
+        else if (mt == 32 && !C) PP_ZL(C, G, 32); \
+        else PP_ZL(C, G, 0);           \
+    } while (0)
+    if (cplx && a.data_fp32) PP_ZLM(true, true);
+    else if (cplx) PP_ZLM(true, false);
+    else if (a.data_fp32) PP_ZLM(false, true);
+    else PP_ZLM(false, false);
+#undef PP_ZLM
 #undef PP_ZL
     return cudaGetLastError();
 }
