@@ -61,6 +61,7 @@ typedef struct pp_solver_s* pp_handle;
 typedef struct {
     int zsolve_lanes; /* lanes sharing one z system: 1..32, a power of two */
     int line_tile;    /* lines per CTA of the generic (non-power-of-two) transform kernel, 1..32 */
+    int zsolve_tile;  /* z systems (adjacent kx) per CTA of the z solve: 1..32, a power of two */
 } pp_tuning;
 
 /* runtime options; the reference keeps these as compile-time switches in
@@ -169,9 +170,9 @@ int pp_workspace_bytes(pp_handle h, size_t* bytes);
 int pp_set_tuning(pp_handle h, const pp_tuning* t);
 int pp_get_tuning(pp_handle h, pp_tuning* t);
 /* autotuner, no counterpart in the reference: times 'reps' solves of the
- * assigned RHS for each candidate lane count of the z solve and, when x or y
- * is not a power of two, each line tile of the generic transform kernel
- * (one coordinate after the other), keeps the fastest shape in the handle and
+ * assigned RHS for each candidate lane count of the z solve, then each
+ * number of z systems per CTA and, when x or y is not a power of two, each
+ * line tile of the generic transform kernel (one coordinate after the other), keeps the fastest shape in the handle and
  * reports it with its milliseconds per solve.  Synchronises the stream; the
  * handle's solution is overwritten. */
 int pp_autotune(pp_handle h, int reps, pp_tuning* chosen, double* best_ms);

@@ -34,7 +34,7 @@ class Options(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("zsolve_lanes", ctypes.c_int), ("line_tile", ctypes.c_int)]
+    _fields_ = [("zsolve_lanes", ctypes.c_int), ("line_tile", ctypes.c_int), ("zsolve_tile", ctypes.c_int)]
 
 
 class PittPackError(RuntimeError):

@@ -95,7 +95,7 @@ int pp_zsolve_lanes(int nz, bool cplx);
 void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads);
 // the same for a chosen lane count (0 or invalid: the default); the launch
 // must then carry P = that lane count
-void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* threads);
+void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* threads, int systems = 0);
 int pp_zsolve_valid_lanes(int nz, int P);
 size_t pp_zsolve_smem_p(int TS, int nz, bool cplx, int P);
 

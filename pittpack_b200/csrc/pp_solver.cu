@@ -90,7 +90,7 @@ struct pp_solver_s {
     // the solve reads the RHS from ext_rhs and writes P to ext_out
     const double* ext_rhs = nullptr;
     double* ext_out = nullptr;
-    pp_tuning tune{0, 0};  // launch-shape choices (0 = built-in default)
+    pp_tuning tune{0, 0, 0};  // launch-shape choices (0 = built-in default)
     DevBuf psum;   // refined solve: per-plane sums / zero-mode column (nz doubles)
     DevBuf zero1;  // one double 0.0 (eigen table of the zero-mode system)
     DevBuf mgstats;  // multigrid z solve: max cycles, unconverged systems (2 ints)
@@ -475,7 +475,7 @@ int launch_solve(pp_solver_s* h)
     z.ny = ny;
     z.nz = nz;
     int zthreads = 0;
-    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads);
+    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads, h->tune.zsolve_tile);
     z.P = h->tune.zsolve_lanes;
     z.tiles_x = (nx + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
@@ -617,7 +617,7 @@ int launch_mixed(pp_solver_s* h)
     z.ny = ny;
     z.nz = nz;
     int zthreads = 0;
-    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads);
+    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads, h->tune.zsolve_tile);
     z.P = h->tune.zsolve_lanes;
     z.tiles_x = (nx + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
@@ -1136,6 +1136,8 @@ static bool valid_tuning(const pp_solver_s* h, const pp_tuning* t)
 {
     if (t->zsolve_lanes != 0 && !pp_zsolve_valid_lanes(h->nz, t->zsolve_lanes)) return false;
     if (t->line_tile < 0 || t->line_tile > 32) return false;
+    if (t->zsolve_tile != 0 && (t->zsolve_tile < 1 || t->zsolve_tile > 32 || (t->zsolve_tile & (t->zsolve_tile - 1))))
+        return false;
     return true;
 }
 
@@ -1190,7 +1192,7 @@ int pp_autotune(pp_handle h, int reps, pp_tuning* chosen, double* best_ms)
         return PP_CUDA_ERROR;
     }
     const pp_tuning start = h->tune;
-    pp_tuning best{0, 0};
+    pp_tuning best{0, 0, 0};
     double bms = 0.0;
     int rc = time_config(h, best, reps, e0, e1, &bms);
     // z solve: lane counts around the default
@@ -1198,6 +1200,17 @@ int pp_autotune(pp_handle h, int reps, pp_tuning* chosen, double* best_ms)
         if (!pp_zsolve_valid_lanes(h->nz, P)) continue;
         pp_tuning t = best;
         t.zsolve_lanes = P;
+        double ms = 0.0;
+        rc = time_config(h, t, reps, e0, e1, &ms);
+        if (rc == PP_SUCCESS && ms < bms) {
+            bms = ms;
+            best = t;
+        }
+    }
+    // z solve: systems per CTA with the chosen lane count
+    for (int T = 2; T <= 32 && rc == PP_SUCCESS; T *= 2) {
+        pp_tuning t = best;
+        t.zsolve_tile = T;
         double ms = 0.0;
         rc = time_config(h, t, reps, e0, e1, &ms);
         if (rc == PP_SUCCESS && ms < bms) {

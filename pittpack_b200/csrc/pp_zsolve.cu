@@ -532,12 +532,17 @@ size_t pp_zsolve_smem_p(int TS, int nz, bool cplx, int P)
     return zlayout(TS, nz, P, cplx, th).bytes;
 }
 
-// the launch shape for a chosen lane count (0 or invalid: the default)
-void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* threads)
+// the launch shape for a chosen lane count (0 or invalid: the default) and
+// systems per CTA (0: as many as fit ~56 KB of shared memory)
+void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* threads, int systems)
 {
     const int P = pp_zsolve_valid_lanes(nz, lanes) ? lanes : pp_zsolve_lanes(nz, cplx);
     int ts = PP_Z_THREADS / P;
-    while (ts > 1 && pp_zsolve_smem_p(ts, nz, cplx, P) > 56 * 1024) ts >>= 1;
+    if (systems >= 1 && (systems & (systems - 1)) == 0 && systems <= ts) {
+        ts = systems;
+        while (ts > 1 && pp_zsolve_smem_p(ts, nz, cplx, P) > 200 * 1024) ts >>= 1;
+    }
+    while (ts > 1 && systems == 0 && pp_zsolve_smem_p(ts, nz, cplx, P) > 56 * 1024) ts >>= 1;
     while (ts > 1 && ts > nx) ts >>= 1;
     *TS = ts;
     *threads = ts * P < 32 ? 32 : ts * P;

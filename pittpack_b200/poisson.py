@@ -168,14 +168,14 @@ class PoissonGPU:
         assert out.dtype == np.complex128 and out.flags.c_contiguous and out.size == self.nx * self.ny * self.nz
         check(self._L.pp_get_solution_async(self._h, out.ctypes.data), "pp_get_solution_async")
 
-    def setTuning(self, zsolve_lanes: int = 0, line_tile: int = 0) -> None:
-        t = _lib.Tuning(int(zsolve_lanes), int(line_tile))
+    def setTuning(self, zsolve_lanes: int = 0, line_tile: int = 0, zsolve_tile: int = 0) -> None:
+        t = _lib.Tuning(int(zsolve_lanes), int(line_tile), int(zsolve_tile))
         check(self._L.pp_set_tuning(self._h, ctypes.byref(t)), "pp_set_tuning")
 
     def tuning(self):
         t = _lib.Tuning()
         check(self._L.pp_get_tuning(self._h, ctypes.byref(t)), "pp_get_tuning")
-        return {"zsolve_lanes": t.zsolve_lanes, "line_tile": t.line_tile}
+        return {"zsolve_lanes": t.zsolve_lanes, "line_tile": t.line_tile, "zsolve_tile": t.zsolve_tile}
 
     def autotune(self, reps: int = 3):
         """Time candidate launch shapes on the assigned RHS and keep the
@@ -183,7 +183,7 @@ class PoissonGPU:
         t = _lib.Tuning()
         ms = ctypes.c_double()
         check(self._L.pp_autotune(self._h, int(reps), ctypes.byref(t), ctypes.byref(ms)), "pp_autotune")
-        return {"zsolve_lanes": t.zsolve_lanes, "line_tile": t.line_tile}, ms.value
+        return {"zsolve_lanes": t.zsolve_lanes, "line_tile": t.line_tile, "zsolve_tile": t.zsolve_tile}, ms.value
 
     def setStream(self, stream_ptr: int) -> None:
         check(self._L.pp_set_stream(self._h, ctypes.c_void_p(stream_ptr)), "pp_set_stream")

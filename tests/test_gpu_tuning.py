@@ -38,11 +38,11 @@ def test_every_launch_shape_gives_the_same_solution(shape):
         M.assignRhs(f)
         lanes = [P for P in (1, 2, 4, 8, 16, 32) if P == 1 or P <= nz // 2]
         for P in lanes:
-            for L in (0, 1, 4, 8):
-                M.setTuning(zsolve_lanes=P, line_tile=L)
-                assert M.tuning() == {"zsolve_lanes": P, "line_tile": L}
+            for L, T in ((0, 0), (1, 2), (4, 8), (8, 1), (0, 32)):
+                M.setTuning(zsolve_lanes=P, line_tile=L, zsolve_tile=T)
+                assert M.tuning() == {"zsolve_lanes": P, "line_tile": L, "zsolve_tile": T}
                 M.pittPack()
-                assert _rel(M.getSolution(), Q) <= TOL, (P, L)
+                assert _rel(M.getSolution(), Q) <= TOL, (P, L, T)
 
 
 def test_autotune_keeps_a_valid_shape_and_the_result():
@@ -65,7 +65,8 @@ def test_invalid_tuning_is_rejected():
     import pittpack_b200 as pp
 
     with pp.make_Poisson(16, 16, 8) as M:
-        for bad in ({"zsolve_lanes": 3}, {"zsolve_lanes": 8}, {"zsolve_lanes": 64}, {"line_tile": 33}):
+        for bad in ({"zsolve_lanes": 3}, {"zsolve_lanes": 8}, {"zsolve_lanes": 64}, {"line_tile": 33},
+                    {"zsolve_tile": 3}, {"zsolve_tile": 64}):
             with pytest.raises(pp.PittPackError) as e:
                 M.setTuning(**bad)
             assert e.value.code == 19
