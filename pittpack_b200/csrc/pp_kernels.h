@@ -33,6 +33,12 @@ struct PPLinePassArgs {
     long elem_stride;  // strides in elements (complex elements count once)
     long line_stride;
     long plane_stride;
+    // power-of-two kernel only: the tile of lines l0.. starts at
+    // plane * plane_stride + l0 * tile_stride (0: l0 * line_stride), and the
+    // output may use its own strides (o_*; o_elem_stride = 0: the input's).
+    // This lets the y passes write / read the z-tiled spectrum layout.
+    long tile_stride;
+    long o_elem_stride, o_line_stride, o_plane_stride, o_tile_stride;
     int L;             // lines per CTA tile
     int tiles_per_plane;
     PPFftPlan fft;     // length n, or n/2 for the quarter-wave families
@@ -87,6 +93,8 @@ struct PPZArgs {
     int P;              // lanes per system (0: the default for nz)
     int data_fp32;      // spectrum stored as float / float2 (solved in FP64)
     int skip_zero;      // write zeros for the kx = ky = 0 column
+    int tiled;          // spectrum in the z-tiled layout: tile (ky, kx / TS) is the
+                        // contiguous block [k][kx % TS] at (ky (nx / TS) + kx / TS) nz TS
 };
 
 // lanes that share one z system (a power of two <= 32)

@@ -356,18 +356,27 @@ int pick_lines_fp32(int nfft)
 // whether every contiguous run of a transform tile starts on a 16-byte
 // boundary: the source pointer and the plane / line (contiguous pass) or
 // element (strided pass) strides, in bytes
-int runs_aligned16(const PPLinePassArgs& a, bool strided, size_t elem_bytes)
+int runs_aligned16(const PPLinePassArgs& a, bool strided, size_t elem_bytes, int dl)
 {
     if (reinterpret_cast<uintptr_t>(a.src) % 16) return 0;
     const size_t st = strided ? (size_t)a.elem_stride : (size_t)a.line_stride;
-    return ((size_t)a.plane_stride * elem_bytes) % 16 == 0 && (st * elem_bytes) % 16 == 0;
+    const size_t ts = a.tile_stride ? (size_t)a.tile_stride : (size_t)a.line_stride;  // per line of l0
+    return ((size_t)a.plane_stride * elem_bytes) % 16 == 0 && (st * elem_bytes) % 16 == 0 &&
+           ((size_t)dl * ts * elem_bytes) % 16 == 0;
 }
 
 // one transform pass: the register-resident kernel for power-of-two lengths,
-// the generic shared-memory Stockham kernel otherwise
+// the generic shared-memory Stockham kernel otherwise (which uses the input
+// strides for its output too: it never sees the z-tiled layout)
 cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool strided, bool in_cplx,
                       bool out_cplx, cudaStream_t st, bool fp32 = false)
 {
+    if (a.o_elem_stride == 0) {
+        a.o_elem_stride = a.elem_stride;
+        a.o_line_stride = a.line_stride;
+        a.o_plane_stride = a.plane_stride;
+        a.o_tile_stride = a.tile_stride;
+    }
     const int lpc = pp_lp2_lpc(d.n);
     if (fp32 && lpc == 0) {
         a.fft = d.fft;
@@ -377,29 +386,60 @@ cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool s
         a.tiles_per_plane = (a.nlines + a.L - 1) / a.L;
         return pp_launch_line_pass(a, inverse, strided, in_cplx, out_cplx, st, true);
     }
-    if (fp32) {
-        a.tw = d.twf.p;
-        a.cs2 = d.csf.p;
-        a.in_cplx = in_cplx;
-        a.out_cplx = out_cplx;
-        a.vec16 = runs_aligned16(a, strided, (in_cplx ? 2 : 1) * sizeof(float));
-        const int dl = d.kind == PP_KIND_FFT ? lpc : 2 * lpc;
-        a.L = dl;
-        a.tiles_per_plane = (a.nlines + dl - 1) / dl;
-        return pp_launch_line_pass_pow2<float, float, float>(a, inverse, strided, st);
-    }
     if (lpc > 0) {
-        a.tw = d.tw.p;
-        a.cs2 = d.cs.p;
+        const int dl = d.kind == PP_KIND_FFT ? lpc : 2 * lpc;
+        a.tw = fp32 ? d.twf.p : d.tw.p;
+        a.cs2 = fp32 ? d.csf.p : d.cs.p;
         a.in_cplx = in_cplx;
         a.out_cplx = out_cplx;
-        a.vec16 = runs_aligned16(a, strided, (in_cplx ? 2 : 1) * sizeof(double));
-        const int dl = d.kind == PP_KIND_FFT ? lpc : 2 * lpc;
+        a.vec16 = runs_aligned16(a, strided, (in_cplx ? 2 : 1) * (fp32 ? sizeof(float) : sizeof(double)), dl);
         a.L = dl;
         a.tiles_per_plane = (a.nlines + dl - 1) / dl;
-        return pp_launch_line_pass_pow2<double, double, double>(a, inverse, strided, st);
+        return fp32 ? pp_launch_line_pass_pow2<float, float, float>(a, inverse, strided, st)
+                    : pp_launch_line_pass_pow2<double, double, double>(a, inverse, strided, st);
     }
     return pp_launch_line_pass(a, inverse, strided, in_cplx, out_cplx, st);
+}
+
+// strides of the z-tiled spectrum for the y passes: line kx of plane k at
+// row ky is at ky (nx nz) + (kx / TS) (nz TS) + k TS + kx % TS; a y tile of
+// TS lines starting at l0 (a multiple of TS) begins at k TS + l0 nz
+void set_z_tiled_out(PPLinePassArgs& a, int nx, int nz, int ts)
+{
+    a.o_elem_stride = (long)nx * nz;
+    a.o_line_stride = 1;
+    a.o_plane_stride = ts;
+    a.o_tile_stride = nz;
+}
+void set_z_tiled_in(PPLinePassArgs& a, int nx, int nz, int ts)
+{
+    a.o_elem_stride = a.elem_stride;  // the output keeps the usual layout
+    a.o_line_stride = a.line_stride;
+    a.o_plane_stride = a.plane_stride;
+    a.o_tile_stride = 0;
+    a.elem_stride = (long)nx * nz;
+    a.line_stride = 1;
+    a.plane_stride = ts;
+    a.tile_stride = nz;
+}
+
+// Width of the z-tiled spectrum layout for this solve, 0 for the usual one.
+// The forward y pass writes, and the inverse y pass reads, the spectrum as
+// contiguous z tiles (TS adjacent kx x all nz of one ky), so that the z solve
+// moves whole contiguous blocks; TS is the y pass's lines per tile.  Used
+// when the y pass is the power-of-two kernel with full tiles (nx a multiple
+// of TS), the z solve is the direct one and takes TS systems per CTA.
+int z_tile_width(const pp_solver_s* h, bool s_cplx)
+{
+    if (h->opt.z_solver != PP_ZSOLVE_DIRECT) return 0;
+    const int lpc = pp_lp2_lpc(h->ny);
+    if (lpc == 0) return 0;
+    const int dl = s_cplx ? lpc : 2 * lpc;
+    if (dl < 2 || dl > 16 || h->nx % dl != 0) return 0;
+    if (h->tune.zsolve_tile != 0 && h->tune.zsolve_tile != dl) return 0;
+    int ts = 0, threads = 0;
+    pp_zsolve_config_p(h->nz, s_cplx, h->nx, h->tune.zsolve_lanes, &ts, &threads, dl);
+    return ts == dl ? dl : 0;
 }
 
 // lines per tile of the generic transform kernel: the tuned value when it fits
@@ -464,6 +504,8 @@ int launch_solve(pp_solver_s* h)
     PPLinePassArgs a2 = ay;
     a2.src = h->bufA.as<double>();
     a2.dst = h->bufB.as<double>();
+    const int zt = z_tile_width(h, s_cplx);
+    if (zt) set_z_tiled_out(a2, nx, nz, zt);
     t0 = stamp(h);
     if ((e = line_pass(a2, h->ty, false, true, x_cplx, s_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_Y);
@@ -475,8 +517,9 @@ int launch_solve(pp_solver_s* h)
     z.ny = ny;
     z.nz = nz;
     int zthreads = 0;
-    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads, h->tune.zsolve_tile);
+    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile);
     z.P = h->tune.zsolve_lanes;
+    z.tiled = zt ? 1 : 0;
     z.tiles_x = (nx + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
     z.ay = h->ty.eig.as<double>();
@@ -518,6 +561,7 @@ int launch_solve(pp_solver_s* h)
     PPLinePassArgs a3 = ay;
     a3.src = h->bufB.as<double>();
     a3.dst = h->bufA.as<double>();
+    if (zt) set_z_tiled_in(a3, nx, nz, zt);
     t0 = stamp(h);
     if ((e = line_pass(a3, h->ty, true, true, s_cplx, s_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_Y);
@@ -609,6 +653,7 @@ int launch_mixed(pp_solver_s* h)
     ay.elem_stride = nx;
     ay.line_stride = 1;
 
+    const int zt = z_tile_width(h, s_cplx);
     PPZArgs z{};
     z.data = reinterpret_cast<double*>(B32);
     z.data_fp32 = 1;
@@ -617,8 +662,9 @@ int launch_mixed(pp_solver_s* h)
     z.ny = ny;
     z.nz = nz;
     int zthreads = 0;
-    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads, h->tune.zsolve_tile);
+    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile);
     z.P = h->tune.zsolve_lanes;
+    z.tiled = zt ? 1 : 0;
     z.tiles_x = (nx + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
     z.ay = h->ty.eig.as<double>();
@@ -635,6 +681,7 @@ int launch_mixed(pp_solver_s* h)
     z0.skip_zero = 0;
     z0.nx = 1;
     z0.P = 0;
+    z0.tiled = 0;
     z0.ny = 1;
     pp_zsolve_config(nz, false, 1, &z0.TS, &zthreads);
     z0.tiles_x = 1;
@@ -669,6 +716,7 @@ int launch_mixed(pp_solver_s* h)
         PPLinePassArgs a2 = ay;
         a2.src = reinterpret_cast<const double*>(A32);
         a2.dst = reinterpret_cast<double*>(B32);
+        if (zt) set_z_tiled_out(a2, nx, nz, zt);
         t0 = stamp(h);
         if ((e = line_pass(a2, h->ty, false, true, x_cplx, s_cplx, h->stream, true)) != cudaSuccess)
             return set_cuda_error(h, e, PP_CUFFT_FAIL_Y);
@@ -679,6 +727,7 @@ int launch_mixed(pp_solver_s* h)
         PPLinePassArgs a3 = ay;
         a3.src = reinterpret_cast<const double*>(B32);
         a3.dst = reinterpret_cast<double*>(A32);
+        if (zt) set_z_tiled_in(a3, nx, nz, zt);
         t0 = stamp(h);
         if ((e = line_pass(a3, h->ty, true, true, s_cplx, s_cplx, h->stream, true)) != cudaSuccess)
             return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_Y);

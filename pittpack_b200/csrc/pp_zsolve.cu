@@ -151,8 +151,10 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     const int ts = min(a.TS, nx - kx0);
     T* g = reinterpret_cast<T*>(a.data);
     T32* g32 = reinterpret_cast<T32*>(a.data);
-    const long plane = (long)nx * ny;
-    const long col0 = (long)ky * nx + kx0;
+    // row k of system s at k * plane + col0 + s: the usual [k][ky][kx] layout,
+    // or the z-tiled one, where this CTA's tile is one contiguous block
+    const long plane = a.tiled ? (long)a.TS : (long)nx * ny;
+    const long col0 = a.tiled ? (long)blockIdx.x * nz * a.TS : (long)ky * nx + kx0;
 
     // ---- load the tile asynchronously (thread -> (system, row) without division:
     //      TS is a power of two) and build the pivot tables while it lands ------------
