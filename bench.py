@@ -62,19 +62,37 @@ FALLBACK_HBM_GBS = 6650.0
 KERNEL_NAMES = ["x_forward", "y_forward", "z_solve", "y_inverse", "x_inverse", "residual"]
 
 
-def kernel_bytes_per_point(bc: str, rhs_complex: bool = False, sweeps: int = -1):
+LP2_LPC = {16: 16, 32: 16, 64: 8, 128: 8, 256: 4, 512: 4, 1024: 2, 2048: 1}
+
+
+def half_cols(n: int, bc: str, rhs_complex: bool = False) -> float:
+    """Fraction of the nx spectrum columns the solve keeps: periodic x with a
+    real RHS keeps the half spectra (nx/2 + 1 columns rounded up to the y
+    pass's lines per tile), as the library does; 1 otherwise."""
+    if bc[0:2] != "PP" or rhs_complex or n < 32 or n not in LP2_LPC:
+        return 1.0
+    lpy = LP2_LPC.get(n, 0)
+    q = min(16, (lpy if bc[2:4] == "PP" else 2 * lpy)) if lpy else 1
+    c = -(-(n // 2 + 1) // q) * q
+    return c / n if c <= n else 1.0
+
+
+def kernel_bytes_per_point(bc: str, rhs_complex: bool = False, sweeps: int = -1, n: int = 512):
     """Algorithmic bytes per point of each stage.  sweeps < 0: the plain FP64
     solve; sweeps >= 0: the refined solve (FP32 spectra), summed over its
-    sweeps + 1 passes; the residual stage reads f and u (FP64) and writes r (FP32)."""
+    sweeps + 1 passes; the residual stage reads f and u (FP64) and writes r (FP32).
+    A periodic x spectrum of a real RHS is kept as half spectra (fraction h of
+    the columns), so everything between the x passes moves h times the bytes."""
     x_c = bc[0:2] == "PP"
     s_c = bc[2:4] == "PP"
+    h = half_cols(n, bc, rhs_complex)
     if sweeps < 0:
         r = 16 if rhs_complex else 8
-        X = 16 if x_c else 8
-        S = 16 if s_c else 8
+        X = (16 if x_c else 8) * h
+        S = (16 if s_c else 8) * h
         return [r + X, X + S, 2 * S, 2 * S, S + 16, 0]
-    X = 8 if x_c else 4
-    S = 8 if s_c else 4
+    X = (8 if x_c else 4) * h
+    S = (8 if s_c else 4) * h
     per = [4 + X, X + S, 2 * S, 2 * S, S + 8 + 8, 0]
     tot = [p * (sweeps + 1) for p in per]
     # residual: sweep 0 reads f and writes r; later sweeps also read u; the
@@ -508,7 +526,7 @@ def run_ours(args):
         solves = 0
         for (k_ms, cnt), bc in zip(stages, FAMILIES):
             kern_total += k_ms
-            kern_bytes += np.array(kernel_bytes_per_point(bc, sweeps=sweeps)) * npts * cnt
+            kern_bytes += np.array(kernel_bytes_per_point(bc, sweeps=sweeps, n=n)) * npts * cnt
             solves += cnt
         dom = int(np.argmax(kern_total))
         launches_dom = solves * (1 if sweeps < 0 else sweeps + 1)

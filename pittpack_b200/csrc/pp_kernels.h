@@ -54,6 +54,8 @@ struct PPLinePassArgs {
     const void* cs2;   // family twiddles in the kernel's precision
     int in_cplx, out_cplx;
     int vec16;          // power-of-two kernel: src and its run starts are 16-byte aligned
+    int half;           // power-of-two periodic x pass of a real RHS on half spectra
+                        // (N/2 + 1 complex per line): forward real -> half, inverse half -> real
     // refinement epilogue of the inverse x pass (acc != null): the real part v
     // of each output becomes u = acc + out_scale v + zplane[plane] in FP64;
     // written to acc, or (dst != null) as the final complex-interleaved P

@@ -31,7 +31,16 @@
 
 namespace pp_lp2 {
 
-enum Fam : int { F_DST2 = 0, F_DCT2 = 1, F_FFT = 2, F_Q4 = 3 };
+// F_R2C / F_C2R: the periodic x pass of a real RHS on half spectra (k <= N/2,
+// the other half is the conjugate mirror): two real lines per complex FFT
+enum Fam : int { F_DST2 = 0, F_DCT2 = 1, F_FFT = 2, F_Q4 = 3, F_R2C = 4, F_C2R = 5 };
+
+// raw tile of a family: complex elements (FFT, half-spectrum input) or real;
+// elements per line in the contiguous pass (half spectra: N/2 + 1)
+template <int FAM>
+constexpr bool raw_cplx() { return FAM == F_FFT || FAM == F_C2R; }
+template <int FAM, int N>
+constexpr int raw_len() { return FAM == F_C2R ? N / 2 + 1 : N; }
 
 template <typename T>
 struct Vec2;
@@ -91,8 +100,9 @@ constexpr size_t smem_bytes()
     constexpr size_t a1 = (size_t)LPC * rp_pitch(N) * sizeof(C);
     constexpr size_t a4 = (size_t)2 * LPC * rp_pitch(N / 2) * sizeof(C);
     constexpr size_t lines = a1 > a4 ? a1 : a4;
-    constexpr size_t re = FAM == F_FFT ? sizeof(C) : sizeof(Real);
-    constexpr size_t raw = (size_t)N * (STRIDED ? raw_row_pitch<FAM, LPC>((int)re) : (FAM == F_FFT ? LPC : 2 * LPC)) * re;
+    constexpr size_t re = raw_cplx<FAM>() ? sizeof(C) : sizeof(Real);
+    constexpr size_t raw = (size_t)raw_len<FAM, N>() *
+                           (STRIDED ? raw_row_pitch<FAM, LPC>((int)re) : (FAM == F_FFT ? LPC : 2 * LPC)) * re;
     return lines > raw ? lines : raw;
 }
 
@@ -120,12 +130,16 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     using C = typename Vec2<Real>::type;
     constexpr bool FFTK = FAM == F_FFT;
     constexpr bool Q4 = FAM == F_Q4;
+    constexpr bool R2C = FAM == F_R2C;
+    constexpr bool C2R = FAM == F_C2R;
+    constexpr bool RAWC = raw_cplx<FAM>();
+    constexpr int LLEN = raw_len<FAM, N>();  // raw elements per line
     constexpr int NT = LPC * N / 8;
     constexpr int DL = FFTK ? LPC : 2 * LPC;  // data lines per tile
     constexpr int LN = rp_log2(N);
     constexpr int LDL = rp_log2(DL);
     // raw tile elements: complex for the FFT family, real otherwise
-    using RE = typename std::conditional<FFTK, C, Real>::type;
+    using RE = typename std::conditional<RAWC, C, Real>::type;
     extern __shared__ __align__(16) unsigned char lp2_smem[];
     C* sb = reinterpret_cast<C*>(lp2_smem);
     RE* raw = reinterpret_cast<RE*>(lp2_smem);
@@ -147,32 +161,35 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     const C* cs = reinterpret_cast<const C*>(a.cs2);
     // raw position of (line l, element e)
     constexpr int RP = raw_row_pitch<FAM, LPC>((int)sizeof(RE));
-    auto ridx = [](int l, int e) -> int { return STRIDED ? e * RP + l : l * N + e; };
+    auto ridx = [](int l, int e) -> int { return STRIDED ? e * RP + l : l * LLEN + e; };
 
     // ---- 1. load the raw tile ----------------------------------------------------------
     // full tiles whose global element type equals the raw one go in 16-byte
     // chunks (a line of N elements, or a row segment of DL elements); the
     // rest element by element (real <-> complex conversion, partial tiles)
-    const bool same = FFTK ? (a.in_cplx != 0) : (a.in_cplx == 0);
-    constexpr int RUN = STRIDED ? DL : N;            // elements per contiguous run
+    const bool same = RAWC ? (a.in_cplx != 0) : (a.in_cplx == 0);
+    constexpr int RUN = STRIDED ? DL : LLEN;         // elements per contiguous run
     constexpr int PER = 16 / (int)sizeof(RE);        // elements per 16-byte chunk
     constexpr bool VOK = (RUN * (int)sizeof(RE)) % 16 == 0;  // runs are whole chunks
     if (VOK && same && a.vec16 && nl == DL) {
         constexpr int CPR = VOK ? RUN / PER : 1;     // chunks per run
-        constexpr int TOT = (STRIDED ? N : DL) * CPR;
+        constexpr int TOT = (STRIDED ? LLEN : DL) * CPR;
         const RE* src = reinterpret_cast<const RE*>(a.src);
         for (int c = tid; c < TOT; c += NT) {
             const int r = c / CPR;  // run: element row (strided) or line
             const int k = (c - r * CPR) * PER;
             const long goff = base + (STRIDED ? (long)r * a.elem_stride : (long)r * a.line_stride) + k;
-            cp_async<16>(raw + r * (STRIDED ? RP : N) + k, src + goff);
+            cp_async<16>(raw + r * (STRIDED ? RP : LLEN) + k, src + goff);
         }
     } else {
-        for (int idx = tid; idx < DL * N; idx += NT) {
+        for (int idx = tid; idx < DL * LLEN; idx += NT) {
             int l, e;
             if (STRIDED) {
                 l = idx & (DL - 1);
                 e = idx >> LDL;
+            } else if (C2R) {
+                l = idx / LLEN;
+                e = idx - l * LLEN;
             } else {
                 l = idx >> LN;
                 e = idx & (N - 1);
@@ -181,7 +198,7 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
             if (l < nl) {
                 const long off = base + (long)l * a.line_stride + (long)e * a.elem_stride;
                 const Real* s = reinterpret_cast<const Real*>(a.src);
-                if (FFTK) {
+                if (RAWC) {
                     if (a.in_cplx) {
                         cp_async<2 * sizeof(Real)>(d, s + 2 * off);
                     } else {
@@ -194,7 +211,7 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                 }
             } else {
                 d[0] = (Real)0;
-                if (FFTK) d[1] = (Real)0;
+                if (RAWC) d[1] = (Real)0;
             }
         }
     }
@@ -239,6 +256,33 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     if constexpr (FFTK) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) v[q] = raw[ridx(fl, t + q * (N / 8))];
+    } else if constexpr (R2C) {
+        // two real lines as one complex line z = x_a + i x_b
+        const int la = 2 * fl, lb = la + 1;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int m = t + q * (N / 8);
+            if (STRIDED) v[q] = *reinterpret_cast<const C*>(raw + ridx(la, m));
+            else v[q] = mkc<C>(raw[ridx(la, m)], raw[ridx(lb, m)]);
+        }
+    } else if constexpr (C2R) {
+        // Z_m = X_a,m + i X_b,m with the upper half rebuilt as the conjugate
+        // mirror X_m = conj X_{N-m} of the stored half spectra
+        const int la = 2 * fl, lb = la + 1;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int m = t + q * (N / 8);
+            C xa, xb;
+            if (q < 4 || (q == 4 && t == 0)) {
+                xa = raw[ridx(la, m)];
+                xb = raw[ridx(lb, m)];
+            } else {
+                const C ya = raw[ridx(la, N - m)], yb = raw[ridx(lb, N - m)];
+                xa = mkc<C>(ya.x, -ya.y);
+                xb = mkc<C>(yb.x, -yb.y);
+            }
+            v[q] = mkc<C>(xa.x - xb.y, xa.y + xb.x);
+        }
     } else if constexpr (Q4) {
         // z_m = (x[2m] + i x[N-1-2m]) e^{-i pi m / N}; DST-IV reverses its input
         const bool rev = a.kind == PP_KIND_DST4;
@@ -333,6 +377,53 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
             if (l >= nl) continue;
             const C z = sb[l * P1 + rp_pad(e)];
             put<Real>(a, goff(l, e), plane, z.x, z.y, sc);
+        }
+    } else if constexpr (R2C) {
+        // half spectra k = 0..N/2 of both packed lines:
+        // X_a,k = (Z_k + conj Z_{N-k}) / 2, X_b,k = (Z_k - conj Z_{N-k}) / (2i)
+        constexpr int LL = rp_log2(LPC);
+        for (int idx = tid; idx < LPC * (N / 2); idx += NT) {
+            int cl, kk;
+            if (STRIDED) {
+                cl = idx & (LPC - 1);
+                kk = idx >> LL;
+            } else {
+                cl = idx >> (LN - 1);
+                kk = idx & (N / 2 - 1);
+            }
+            const int la = 2 * cl, lb = la + 1;
+            const C* ln = sb + cl * P1;
+            auto emit = [&](int k, C Zk, C Zn) {
+                if (la < nl)
+                    put<Real>(a, goff(la, k), plane, (Real)0.5 * (Zk.x + Zn.x), (Real)0.5 * (Zk.y - Zn.y), sc);
+                if (lb < nl)
+                    put<Real>(a, goff(lb, k), plane, (Real)0.5 * (Zk.y + Zn.y), -(Real)0.5 * (Zk.x - Zn.x), sc);
+            };
+            const C Zk = ln[rp_pad(kk)];
+            if (kk == 0) {
+                const C Zh = ln[rp_pad(N / 2)];
+                emit(0, Zk, Zk);
+                emit(N / 2, Zh, Zh);
+            } else {
+                emit(kk, Zk, ln[rp_pad(N - kk)]);
+            }
+        }
+    } else if constexpr (C2R) {
+        // z = x_a + i x_b: both real lines at once
+        constexpr int LL = rp_log2(LPC);
+        for (int idx = tid; idx < LPC * N; idx += NT) {
+            int cl, e;
+            if (STRIDED) {
+                cl = idx & (LPC - 1);
+                e = idx >> LL;
+            } else {
+                cl = idx >> LN;
+                e = idx & (N - 1);
+            }
+            const int la = 2 * cl, lb = la + 1;
+            const C z = sb[cl * P1 + rp_pad(e)];
+            if (la < nl) put<Real>(a, goff(la, e), plane, z.x, (Real)0, sc);
+            if (lb < nl) put<Real>(a, goff(lb, e), plane, z.y, (Real)0, sc);
         }
     } else if constexpr (Q4) {
         // w_p = e^{-i pi (4p+1)/(4N)} Z_p: X[2p] = c Re w_p, X[N-1-2p] = -c Im w_p
@@ -444,9 +535,25 @@ cudaError_t launch_fam(const PPLinePassArgs& a, bool inverse, bool strided, cuda
 #undef PP_LP2
 }
 
+template <typename Real, int N, int LPC, int FAM>
+cudaError_t launch_half(const PPLinePassArgs& a, cudaStream_t st)
+{
+    // the contiguous x pass only: forward real -> half spectra, inverse back
+    constexpr size_t smem = smem_bytes<Real, N, LPC, FAM, false>();
+    auto kfn = lp2_kernel<Real, N, LPC, FAM, FAM == F_C2R, false>;
+    cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kfn<<<a.nplanes * a.tiles_per_plane, LPC * N / 8, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
 template <typename Real, int N, int LPC>
 cudaError_t launch_n(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
 {
+    if (a.half && a.kind == PP_KIND_FFT) {
+        if (strided) return cudaErrorInvalidValue;
+        return inverse ? launch_half<Real, N, LPC, F_C2R>(a, st) : launch_half<Real, N, LPC, F_R2C>(a, st);
+    }
     switch (a.kind) {
     case PP_KIND_DST2: return launch_fam<Real, N, LPC, F_DST2>(a, inverse, strided, st);
     case PP_KIND_DCT2: return launch_fam<Real, N, LPC, F_DCT2>(a, inverse, strided, st);

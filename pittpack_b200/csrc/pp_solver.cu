@@ -423,23 +423,63 @@ void set_z_tiled_in(PPLinePassArgs& a, int nx, int nz, int ts)
     a.tile_stride = nz;
 }
 
+// the periodic x pass on half spectra: ncol complex columns per row of the
+// spectrum; the forward pass writes there, the inverse pass reads there and
+// writes the usual nx-wide layout
+void set_half_out(PPLinePassArgs& a, int ncol, long splane)
+{
+    a.half = 1;
+    a.o_elem_stride = 1;
+    a.o_line_stride = ncol;
+    a.o_plane_stride = splane;
+    a.o_tile_stride = 0;
+}
+void set_half_in(PPLinePassArgs& a, int ncol, long splane, int nx, long plane)
+{
+    a.half = 1;
+    a.elem_stride = 1;
+    a.line_stride = ncol;
+    a.plane_stride = splane;
+    a.tile_stride = 0;
+    a.o_elem_stride = 1;
+    a.o_line_stride = nx;
+    a.o_plane_stride = plane;
+    a.o_tile_stride = 0;
+}
+
 // Width of the z-tiled spectrum layout for this solve, 0 for the usual one.
 // The forward y pass writes, and the inverse y pass reads, the spectrum as
 // contiguous z tiles (TS adjacent kx x all nz of one ky), so that the z solve
 // moves whole contiguous blocks; TS is the y pass's lines per tile.  Used
 // when the y pass is the power-of-two kernel with full tiles (nx a multiple
 // of TS), the z solve is the direct one and takes TS systems per CTA.
-int z_tile_width(const pp_solver_s* h, bool s_cplx)
+int z_tile_width(const pp_solver_s* h, bool s_cplx, int ncol)
 {
     if (h->opt.z_solver != PP_ZSOLVE_DIRECT) return 0;
     const int lpc = pp_lp2_lpc(h->ny);
     if (lpc == 0) return 0;
     const int dl = s_cplx ? lpc : 2 * lpc;
-    if (dl < 2 || dl > 16 || h->nx % dl != 0) return 0;
+    if (dl < 2 || dl > 16 || ncol % dl != 0) return 0;
     if (h->tune.zsolve_tile != 0 && h->tune.zsolve_tile != dl) return 0;
     int ts = 0, threads = 0;
-    pp_zsolve_config_p(h->nz, s_cplx, h->nx, h->tune.zsolve_lanes, &ts, &threads, dl);
+    pp_zsolve_config_p(h->nz, s_cplx, ncol, h->tune.zsolve_lanes, &ts, &threads, dl);
     return ts == dl ? dl : 0;
+}
+
+// Periodic x with a real RHS: the x spectrum of every line is Hermitian, so
+// only k = 0..nx/2 is kept (the rest is its conjugate mirror, and the
+// eigenvalue is symmetric in kx): the y passes and the z solve then handle
+// ~half the columns.  Columns of the spectrum: nx/2 + 1, rounded up to the
+// y pass's lines per tile (<= 16) so that the z-tiled layout still applies;
+// 0 when the path does not apply (the full complex spectrum is used).
+int half_spectrum_cols(const pp_solver_s* h)
+{
+    if (h->tx.kind != PP_KIND_FFT || h->rhs_complex || h->nx < 32 || pp_lp2_lpc(h->nx) == 0) return 0;
+    const int lpy = pp_lp2_lpc(h->ny);
+    int q = lpy ? (h->ty.kind == PP_KIND_FFT ? lpy : 2 * lpy) : 1;
+    if (q > 16) q = 16;
+    const int c = ((h->nx / 2 + 1 + q - 1) / q) * q;
+    return c <= h->nx ? c : 0;
 }
 
 // lines per tile of the generic transform kernel: the tuned value when it fits
@@ -458,6 +498,10 @@ int launch_solve(pp_solver_s* h)
     const bool s_cplx = ky == PP_KIND_FFT;  // spectrum (after the y transform)
     const double dz = -(h->box[4] - h->box[5]) / (nz);
     const long plane = (long)nx * ny;
+    // spectrum columns: nx, or the half spectra of the periodic x pass
+    const int hc = half_spectrum_cols(h);
+    const int ncol = hc ? hc : nx;
+    const long splane = (long)ncol * ny;
     cudaError_t e;
     int t0;
 
@@ -482,13 +526,14 @@ int launch_solve(pp_solver_s* h)
     PPLinePassArgs ay = ax;
     ay.n = ny;
     ay.kind = ky;
-    ay.nlines = nx;
-    ay.elem_stride = nx;
+    ay.nlines = ncol;
+    ay.elem_stride = ncol;
     ay.line_stride = 1;
+    ay.plane_stride = splane;
     ay.fft = h->ty.fft;
     ay.cs = h->ty.cs.as<double2>();
     ay.L = tuned_lines(h, ay.fft.n);
-    ay.tiles_per_plane = (nx + ay.L - 1) / ay.L;
+    ay.tiles_per_plane = (ncol + ay.L - 1) / ay.L;
 
     // forward x: rhs -> A
     PPLinePassArgs a1 = ax;
@@ -496,6 +541,7 @@ int launch_solve(pp_solver_s* h)
     a1.dst = h->bufA.as<double>();
     a1.rhs_scale = 1;
     a1.lift = h->liftv;
+    if (hc) set_half_out(a1, ncol, splane);
     t0 = stamp(h);
     if ((e = line_pass(a1, h->tx, false, false, h->rhs_complex, x_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_X);
@@ -504,8 +550,8 @@ int launch_solve(pp_solver_s* h)
     PPLinePassArgs a2 = ay;
     a2.src = h->bufA.as<double>();
     a2.dst = h->bufB.as<double>();
-    const int zt = z_tile_width(h, s_cplx);
-    if (zt) set_z_tiled_out(a2, nx, nz, zt);
+    const int zt = z_tile_width(h, s_cplx, ncol);
+    if (zt) set_z_tiled_out(a2, ncol, nz, zt);
     t0 = stamp(h);
     if ((e = line_pass(a2, h->ty, false, true, x_cplx, s_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_Y);
@@ -513,14 +559,14 @@ int launch_solve(pp_solver_s* h)
     // z solve in B
     PPZArgs z{};
     z.data = h->bufB.as<double>();
-    z.nx = nx;
+    z.nx = ncol;
     z.ny = ny;
     z.nz = nz;
     int zthreads = 0;
-    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile);
+    pp_zsolve_config_p(nz, s_cplx, ncol, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile);
     z.P = h->tune.zsolve_lanes;
     z.tiled = zt ? 1 : 0;
-    z.tiles_x = (nx + z.TS - 1) / z.TS;
+    z.tiles_x = (ncol + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
     z.ay = h->ty.eig.as<double>();
     const double dx = -(h->box[0] - h->box[1]) / (nx);
@@ -538,7 +584,7 @@ int launch_solve(pp_solver_s* h)
             return set_cuda_error(h, e, PP_CUDA_ERROR);
         PPZMgArgs m{};
         m.data = z.data;
-        m.nx = nx;
+        m.nx = ncol;
         m.ny = ny;
         m.nz = nz;
         m.ax = z.ax;
@@ -561,7 +607,7 @@ int launch_solve(pp_solver_s* h)
     PPLinePassArgs a3 = ay;
     a3.src = h->bufB.as<double>();
     a3.dst = h->bufA.as<double>();
-    if (zt) set_z_tiled_in(a3, nx, nz, zt);
+    if (zt) set_z_tiled_in(a3, ncol, nz, zt);
     t0 = stamp(h);
     if ((e = line_pass(a3, h->ty, true, true, s_cplx, s_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_Y);
@@ -571,6 +617,7 @@ int launch_solve(pp_solver_s* h)
     a4.src = h->bufA.as<double>();
     a4.dst = h->ext_out ? h->ext_out : h->out.as<double>();
     a4.out_scale = 1. / ((double)(nx * ny));
+    if (hc) set_half_in(a4, ncol, splane, nx, plane);
     t0 = stamp(h);
     if ((e = line_pass(a4, h->tx, true, false, s_cplx, true, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_X);
@@ -602,6 +649,10 @@ int launch_mixed(pp_solver_s* h)
     const double dx = -(h->box[0] - h->box[1]) / (nx);
     const double dy = -(h->box[2] - h->box[3]) / (ny);
     const long plane = (long)nx * ny;
+    // spectrum columns: nx, or the half spectra of the periodic x pass
+    const int hc = half_spectrum_cols(h);
+    const int ncol = hc ? hc : nx;
+    const long splane = (long)ncol * ny;
     cudaError_t e;
     int t0;
     if (h->rhs_complex || h->opt.z_solver != PP_ZSOLVE_DIRECT) return PP_UNSUPPORTED;
@@ -649,23 +700,24 @@ int launch_mixed(pp_solver_s* h)
     PPLinePassArgs ay = ax;
     ay.n = ny;
     ay.kind = ky;
-    ay.nlines = nx;
-    ay.elem_stride = nx;
+    ay.nlines = ncol;
+    ay.elem_stride = ncol;
     ay.line_stride = 1;
+    ay.plane_stride = splane;
 
-    const int zt = z_tile_width(h, s_cplx);
+    const int zt = z_tile_width(h, s_cplx, ncol);
     PPZArgs z{};
     z.data = reinterpret_cast<double*>(B32);
     z.data_fp32 = 1;
     z.skip_zero = zm ? 1 : 0;
-    z.nx = nx;
+    z.nx = ncol;
     z.ny = ny;
     z.nz = nz;
     int zthreads = 0;
-    pp_zsolve_config_p(nz, s_cplx, nx, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile);
+    pp_zsolve_config_p(nz, s_cplx, ncol, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile);
     z.P = h->tune.zsolve_lanes;
     z.tiled = zt ? 1 : 0;
-    z.tiles_x = (nx + z.TS - 1) / z.TS;
+    z.tiles_x = (ncol + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
     z.ay = h->ty.eig.as<double>();
     z.Cx = ra.Cx;
@@ -709,6 +761,7 @@ int launch_mixed(pp_solver_s* h)
         PPLinePassArgs a1 = ax;
         a1.src = reinterpret_cast<const double*>(r32);
         a1.dst = reinterpret_cast<double*>(A32);
+        if (hc) set_half_out(a1, ncol, splane);
         t0 = stamp(h);
         if ((e = line_pass(a1, h->tx, false, false, false, x_cplx, h->stream, true)) != cudaSuccess)
             return set_cuda_error(h, e, PP_CUFFT_FAIL_X);
@@ -716,7 +769,7 @@ int launch_mixed(pp_solver_s* h)
         PPLinePassArgs a2 = ay;
         a2.src = reinterpret_cast<const double*>(A32);
         a2.dst = reinterpret_cast<double*>(B32);
-        if (zt) set_z_tiled_out(a2, nx, nz, zt);
+        if (zt) set_z_tiled_out(a2, ncol, nz, zt);
         t0 = stamp(h);
         if ((e = line_pass(a2, h->ty, false, true, x_cplx, s_cplx, h->stream, true)) != cudaSuccess)
             return set_cuda_error(h, e, PP_CUFFT_FAIL_Y);
@@ -727,7 +780,7 @@ int launch_mixed(pp_solver_s* h)
         PPLinePassArgs a3 = ay;
         a3.src = reinterpret_cast<const double*>(B32);
         a3.dst = reinterpret_cast<double*>(A32);
-        if (zt) set_z_tiled_in(a3, nx, nz, zt);
+        if (zt) set_z_tiled_in(a3, ncol, nz, zt);
         t0 = stamp(h);
         if ((e = line_pass(a3, h->ty, true, true, s_cplx, s_cplx, h->stream, true)) != cudaSuccess)
             return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_Y);
@@ -740,6 +793,7 @@ int launch_mixed(pp_solver_s* h)
         a4.zplane = zm ? h->psum.as<double>() : nullptr;
         a4.zscale = 1.0 / (ra.psum_scale * (double)nx * (double)ny);
         a4.out_scale = 1. / ((double)(nx * ny));
+        if (hc) set_half_in(a4, ncol, splane, nx, plane);
         t0 = stamp(h);
         if ((e = line_pass(a4, h->tx, true, false, s_cplx, false, h->stream, true)) != cudaSuccess)
             return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_X);
