@@ -41,48 +41,56 @@ PP_D double lift3(const PPLift& L, int i, int j, int k, int nx, int ny, int nz)
 // neighbour across a face: code 0 Dirichlet (-u), 1 Neumann (+u), 2 periodic
 PP_D double ghost(int code, double uc, double uw) { return code == 2 ? uw : (code == 1 ? uc : -uc); }
 
+// One CTA per (group of RESID_ROWS rows j, plane k): its threads walk each
+// row with stride blockDim, so that the plane sums need one atomic per CTA
+// (a few per plane) rather than one per half row.
+constexpr int RESID_ROWS = 16;
+
 __global__ void __launch_bounds__(256) resid_kernel(PPResidArgs a)
 {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    const int k = blockIdx.z;
-    double r = 0.0;
-    if (i < nx) {
-        const long plane = (long)nx * ny;
+    const int k = blockIdx.y;
+    const int j0 = blockIdx.x * RESID_ROWS;
+    const int rows = min(RESID_ROWS, ny - j0);
+    const long plane = (long)nx * ny;
+    double rs = 0.0, us = 0.0;
+    for (int jj = 0; jj < rows; ++jj)
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const int j = j0 + jj;
         const long p = i + (long)nx * j + plane * k;
         double b = a.f[p] * a.dz * a.dz;
         if (a.lift.any) b = b - lift3(a.lift, i, j, k, nx, ny, nz);
+        double r;
         if (a.u) {
             const double* u = a.u;
             const double uc = u[p];
             const double uw = i > 0 ? u[p - 1] : ghost(a.bc[0], uc, u[p + nx - 1]);
             const double ue = i < nx - 1 ? u[p + 1] : ghost(a.bc[1], uc, u[p - (nx - 1)]);
-            const double us = j > 0 ? u[p - nx] : ghost(a.bc[2], uc, u[p + (long)nx * (ny - 1)]);
+            const double us_ = j > 0 ? u[p - nx] : ghost(a.bc[2], uc, u[p + (long)nx * (ny - 1)]);
             const double un = j < ny - 1 ? u[p + nx] : ghost(a.bc[3], uc, u[p - (long)nx * (ny - 1)]);
             const double ub = k > 0 ? u[p - plane] : ghost(a.bc[4], uc, u[p + plane * (nz - 1)]);
             const double ut = k < nz - 1 ? u[p + plane] : ghost(a.bc[5], uc, u[p - plane * (nz - 1)]);
-            const double au = a.Cx * (uw - 2.0 * uc + ue) + a.Cy * (us - 2.0 * uc + un) + (ub - 2.0 * uc + ut);
+            const double au = a.Cx * (uw - 2.0 * uc + ue) + a.Cy * (us_ - 2.0 * uc + un) + (ub - 2.0 * uc + ut);
             r = b - au;
+            if (a.usum) us += uc;
         } else {
             r = b;
         }
         a.r[p] = (float)r;
+        rs += r;
     }
     if (a.psum) {
-        // FP64 plane sum of r (and sum of u): block reduction, one atomic per block
-        double v = r;
-        double uu = (a.usum && i < nx) ? a.u[i + (long)nx * j + (long)nx * ny * k] : 0.0;
+        // FP64 plane sum of r (and sum of u): block reduction, one atomic per CTA
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            v += __shfl_xor_sync(0xffffffffu, v, o);
-            uu += __shfl_xor_sync(0xffffffffu, uu, o);
+            rs += __shfl_xor_sync(0xffffffffu, rs, o);
+            us += __shfl_xor_sync(0xffffffffu, us, o);
         }
         __shared__ double ws[8], wu[8];
         const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
         if (ln == 0) {
-            ws[w] = v;
-            wu[w] = uu;
+            ws[w] = rs;
+            wu[w] = us;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -133,8 +141,7 @@ cudaError_t pp_launch_zero_mode_anchor(double* zcol, int nz, const double* usum,
 
 cudaError_t pp_launch_resid(const PPResidArgs& a, cudaStream_t st)
 {
-    const int bx = a.nx >= 256 ? 256 : ((a.nx + 31) / 32) * 32;
-    dim3 grid((a.nx + bx - 1) / bx, a.ny, a.nz), block(bx);
+    dim3 grid((a.ny + RESID_ROWS - 1) / RESID_ROWS, a.nz), block(256);
     resid_kernel<<<grid, block, 0, st>>>(a);
     return cudaGetLastError();
 }
