@@ -60,6 +60,11 @@ FALLBACK_HBM_GBS = 6650.0
 # algorithmic bytes per point of each solve kernel for a real RHS:
 # (read + write), see DESIGN.md "Kernels and their rooflines"
 KERNEL_NAMES = ["x_forward", "y_forward", "z_solve", "y_inverse", "x_inverse", "residual"]
+# DRAM bytes moved / algorithmic bytes per stage, from one ncu capture of the
+# FP64 solve (512 x 512 x 128, NN family; profiles/solve_kernels_dram_traffic_512x512x128.md):
+# reads equal the algorithmic bytes, writes read low by what is still in L2
+DRAM_OVER_ALGORITHMIC = {"x_forward": 14.67 / 16, "y_forward": 14.53 / 16, "z_solve": 14.08 / 16,
+                         "y_inverse": 14.42 / 16, "x_inverse": 22.14 / 24}
 
 
 LP2_LPC = {16: 16, 32: 16, 64: 8, 128: 8, 256: 4, 512: 4, 1024: 2, 2048: 1}
@@ -138,7 +143,7 @@ class ClockSampler:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -329,7 +334,9 @@ def run_serve_leg(args):
     pts = sum(n ** 3 for n, _ in reqs)
     out = {}
     for name, prec in (("fp64", 0), ("mixed", 1)):
-        S = Server(streams=8, hbm_fraction=0.5)
+        # a budget that holds every warmed shape: no handle is created or
+        # evicted (cudaFree waits for the device) while requests arrive
+        S = Server(streams=8, hbm_fraction=0.85)
         # plans, twiddles and workspaces resident before the stream starts
         seen = set()
         for n, bc in reqs:
@@ -543,7 +550,11 @@ def run_ours(args):
             "value": world * args.steps * len(FAMILIES) * npts / (ms / 1e3) / 1e6,
             "ms_per_solve": solve_ms,
             "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": (per_launch_bytes * DRAM_OVER_ALGORITHMIC[KERNEL_NAMES[dom]]
+                                     if sweeps < 0 and KERNEL_NAMES[dom] in DRAM_OVER_ALGORITHMIC else None),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 512x512x128, "
+                                           "as a ratio to the algorithmic bytes, applied per launch",
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "algorithmic_bytes_per_launch": per_launch_bytes},
             "solve_roofline": {"algorithmic_bytes_per_point": alg / npts,
@@ -673,7 +684,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=N_GRID, help="grid edge (the benchmark uses 512)")
