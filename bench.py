@@ -63,26 +63,26 @@ KERNEL_NAMES = ["x_forward", "y_forward", "z_solve", "y_inverse", "x_inverse", "
 # DRAM bytes moved / algorithmic bytes per stage, from one ncu capture of the
 # FP64 solve (512 x 512 x 128, NN family; profiles/solve_kernels_dram_traffic_512x512x128.md):
 # reads equal the algorithmic bytes, writes read low by what is still in L2
-DRAM_OVER_ALGORITHMIC = {"x_forward": 14.67 / 16, "y_forward": 14.53 / 16, "z_solve": 14.08 / 16,
-                         "y_inverse": 14.42 / 16, "x_inverse": 22.14 / 24}
+DRAM_OVER_ALGORITHMIC = {"x_forward": 14.72 / 16, "y_forward": 14.54 / 16, "z_solve": 14.10 / 16,
+                         "y_inverse": 14.43 / 16, "x_inverse": 22.17 / 24}
 
 
 LP2_LPC = {16: 16, 32: 16, 64: 8, 128: 8, 256: 4, 512: 4, 1024: 2, 2048: 1}
 
 
-def half_cols(n: int, bc: str, rhs_complex: bool = False) -> float:
+def half_cols(n: int, bc: str, rhs_complex: bool = False, ny: int = 0) -> float:
     """Fraction of the nx spectrum columns the solve keeps: periodic x with a
     real RHS keeps the half spectra (nx/2 + 1 columns rounded up to the y
     pass's lines per tile), as the library does; 1 otherwise."""
     if bc[0:2] != "PP" or rhs_complex or n < 32 or n not in LP2_LPC:
         return 1.0
-    lpy = LP2_LPC.get(n, 0)
+    lpy = LP2_LPC.get(ny or n, 0)
     q = min(16, (lpy if bc[2:4] == "PP" else 2 * lpy)) if lpy else 1
     c = -(-(n // 2 + 1) // q) * q
     return c / n if c <= n else 1.0
 
 
-def kernel_bytes_per_point(bc: str, rhs_complex: bool = False, sweeps: int = -1, n: int = 512):
+def kernel_bytes_per_point(bc: str, rhs_complex: bool = False, sweeps: int = -1, n: int = 512, ny: int = 0):
     """Algorithmic bytes per point of each stage.  sweeps < 0: the plain FP64
     solve; sweeps >= 0: the refined solve (FP32 spectra), summed over its
     sweeps + 1 passes; the residual stage reads f and u (FP64) and writes r (FP32).
@@ -90,7 +90,7 @@ def kernel_bytes_per_point(bc: str, rhs_complex: bool = False, sweeps: int = -1,
     the columns), so everything between the x passes moves h times the bytes."""
     x_c = bc[0:2] == "PP"
     s_c = bc[2:4] == "PP"
-    h = half_cols(n, bc, rhs_complex)
+    h = half_cols(n, bc, rhs_complex, ny)
     if sweeps < 0:
         r = 16 if rhs_complex else 8
         X = (16 if x_c else 8) * h
@@ -179,15 +179,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_rhs(torch, bc: str, n: int, seed: int, device):
-    """Seeded sum of 8 eigenmodes of the family plus 1e-3 uniform noise."""
+def make_rhs(torch, bc: str, shape, seed: int, device):
+    """Seeded sum of 8 eigenmodes of the family plus 1e-3 uniform noise;
+    shape = (nx, ny, nz), the array is (nz, ny, nx)."""
+    nx, ny, nz = shape
     g = torch.Generator(device="cpu").manual_seed(seed)
     amps = torch.randn(8, generator=g, dtype=torch.float64)
-    waves = torch.randint(0, n // 4, (8, 3), generator=g)
+    waves = torch.randint(0, min(shape) // 4, (8, 3), generator=g)
     phase = torch.randint(0, 2, (8, 2), generator=g)
-    c = (torch.arange(n, dtype=torch.float64, device=device) + 0.5) / n  # cell centres on [0,1]
+    centres = [(torch.arange(m, dtype=torch.float64, device=device) + 0.5) / m for m in shape]  # on [0,1]
 
-    def mode1d(pair: str, k: int, ph: int):
+    def mode1d(pair: str, k: int, ph: int, c):
         if pair == "PP":
             return torch.cos(2 * torch.pi * k * c) if ph == 0 else torch.sin(2 * torch.pi * k * c)
         if pair == "NN":
@@ -198,12 +200,12 @@ def make_rhs(torch, bc: str, n: int, seed: int, device):
             return torch.cos(torch.pi * (k + 0.5) * c)
         return torch.sin(torch.pi * (k + 0.5) * c)  # DN
 
-    f = torch.zeros((n, n, n), dtype=torch.float64, device=device)
+    f = torch.zeros((nz, ny, nx), dtype=torch.float64, device=device)
     for m in range(8):
         kx, ky, kz = (int(v) for v in waves[m])
-        mx = mode1d(bc[0:2], kx, int(phase[m, 0]))
-        my = mode1d(bc[2:4], ky, int(phase[m, 1]))
-        mz = mode1d(bc[4:6], kz, 0)
+        mx = mode1d(bc[0:2], kx, int(phase[m, 0]), centres[0])
+        my = mode1d(bc[2:4], ky, int(phase[m, 1]), centres[1])
+        mz = mode1d(bc[4:6], kz, 0, centres[2])
         f.add_(float(amps[m]) * mz[:, None, None] * my[None, :, None] * mx[None, None, :])
     gn = torch.Generator(device=device).manual_seed(seed + 1000)
     f.add_((torch.rand(f.shape, generator=gn, dtype=torch.float64, device=device) * 2 - 1) * 1e-3)
@@ -471,16 +473,18 @@ def run_ours(args):
     from pittpack_b200.poisson import pinned_empty
 
     n = args.n
-    npts = n ** 3
+    nx, ny, nz = args.grid if args.grid else (n, n, n)
+    npts = nx * ny * nz
+    FAMILIES = args.families.split(",") if args.families else globals()["FAMILIES"]
     stream = torch.cuda.current_stream()
     solvers, rhs_dev = [], []
     for idx, bc in enumerate(FAMILIES):
-        M = pp.make_Poisson(n, n, n)
+        M = pp.make_Poisson(nx, ny, nz)
         M.assignBoundary(bc)
         M.setBox([0, 1, 0, 1, 0, 1])
         M.setCoords(2)
         M.setStream(stream.cuda_stream)
-        f = make_rhs(torch, bc, n, 3 + idx, torch.device("cuda", local_rank))
+        f = make_rhs(torch, bc, (nx, ny, nz), 3 + idx, torch.device("cuda", local_rank))
         M.assignRhsDevice(f.data_ptr(), False)
         solvers.append(M)
         rhs_dev.append(f)
@@ -533,7 +537,7 @@ def run_ours(args):
         solves = 0
         for (k_ms, cnt), bc in zip(stages, FAMILIES):
             kern_total += k_ms
-            kern_bytes += np.array(kernel_bytes_per_point(bc, sweeps=sweeps, n=n)) * npts * cnt
+            kern_bytes += np.array(kernel_bytes_per_point(bc, sweeps=sweeps, n=nx, ny=ny)) * npts * cnt
             solves += cnt
         dom = int(np.argmax(kern_total))
         launches_dom = solves * (1 if sweeps < 0 else sweeps + 1)
@@ -599,14 +603,14 @@ def run_ours(args):
     # ---- end to end through the public API ---------------------------------------
     h_rhs = []
     for f in rhs_dev:
-        a = pinned_empty((n, n, n), np.float64)
+        a = pinned_empty((nz, ny, nx), np.float64)
         a[...] = f.cpu().numpy()
         h_rhs.append(a)
     del rhs_dev
     # one stream and one page-locked output per grid: the four solves are
     # issued with the asynchronous public calls, so one grid's upload overlaps
     # another's download and compute
-    h_out = [pinned_empty((n, n, n), np.complex128) for _ in solvers]
+    h_out = [pinned_empty((nz, ny, nx), np.complex128) for _ in solvers]
     e2e_streams = [torch.cuda.Stream() for _ in solvers]
     for M, s in zip(solvers, e2e_streams):
         M.setStream(s.cuda_stream)
@@ -657,8 +661,9 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if best == "fp64" else "f32 + f64 refinement",
             "data": "synthetic (seeded eigenmode sums + 1e-3 noise, generated on device)",
-            "config": {"workload": f"{n}^3 grid x 4 x/y families (PPPP, NNNN, NDND, DDDD), Dirichlet z",
-                       "grid": [n, n, n], "families": FAMILIES, "mode": best,
+            "config": {"workload": (f"{nx}^3 grid" if nx == ny == nz else f"{nx}x{ny}x{nz} grid")
+                                   + f" x {len(FAMILIES)} boundary sets ({', '.join(FAMILIES)})",
+                       "grid": [nx, ny, nz], "families": FAMILIES, "mode": best,
                        "l2": "inputs (1 GiB per grid) larger than L2, no flush",
                        "parallelism": f"replicas x{world}"},
             "ms_per_solve": results[best]["ms_per_solve"],
@@ -688,6 +693,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=N_GRID, help="grid edge (the benchmark uses 512)")
+    ap.add_argument("--grid", type=int, nargs=3, metavar=("NX", "NY", "NZ"), help="a non-cubic grid instead of --n")
+    ap.add_argument("--families", type=str, default="", help="comma-separated boundary sets instead of the four")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--sweeps", type=int, default=1, help="refinement sweeps of the mixed-precision mode")
     ap.add_argument("--no-batch", action="store_true", help="skip the 96-grid batched workload")
