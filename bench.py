@@ -115,6 +115,23 @@ def launches_per_solve(bc: str, sweeps: int = -1) -> int:
     return (sweeps + 1) * (6 + int(zm) + int(singular))
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The slowest rank's value (every rank takes this same collective; the
+    replicas exchange nothing else)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, units_per_rank: float, seconds: float) -> float:
+    """Whole-job Mpoints/s of N independent replicas timed by the slowest."""
+    return world * units_per_rank / seconds / 1e6
+
+
 def env_rank():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
             int(os.environ.get("WORLD_SIZE", "1")))
@@ -523,10 +540,8 @@ def run_ours(args):
         clk = clocks.stop()
         ms = t0.elapsed_time(t1)
         stages = [M.timingEnd() for M in solvers]
+        ms = max_over_ranks(ms, dist, "cuda")
         if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
             dist.barrier()
         return ms, stages, clk
 
@@ -551,7 +566,7 @@ def run_ours(args):
                                      "GBps": (kern_bytes[i] / (kern_total[i] / 1e3) / 1e9) if kern_total[i] > 0 else 0.0}
                    for i in range(6) if kern_total[i] > 0}
         return {
-            "value": world * args.steps * len(FAMILIES) * npts / (ms / 1e3) / 1e6,
+            "value": replica_throughput(world, args.steps * len(FAMILIES) * npts, ms / 1e3),
             "ms_per_solve": solve_ms,
             "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
@@ -632,12 +647,8 @@ def run_ours(args):
     for _ in range(e2e_steps):
         e2e_step()
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - w0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_val = world * e2e_steps * len(FAMILIES) * npts / e2e_s / 1e6
+    e2e_s = max_over_ranks(time.perf_counter() - w0, dist, "cuda")
+    e2e_val = replica_throughput(world, e2e_steps * len(FAMILIES) * npts, e2e_s)
 
     for M in solvers:
         M.close()
