@@ -150,13 +150,6 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     const int l0 = (tile - plane * a.tiles_per_plane) * DL;
     const int nl = min(DL, a.nlines - l0);
     const long base = (long)plane * a.plane_stride + (long)l0 * (a.tile_stride ? a.tile_stride : a.line_stride);
-    // output strides: their own (z-tiled spectrum) or, when unset, the input's
-    const bool own = a.o_elem_stride != 0;
-    const long oes = own ? a.o_elem_stride : a.elem_stride;
-    const long ols = own ? a.o_line_stride : a.line_stride;
-    const long ops = own ? a.o_plane_stride : a.plane_stride;
-    const long ots = own ? a.o_tile_stride : a.tile_stride;
-    const long obase = (long)plane * ops + (long)l0 * (ots ? ots : ols);
     const C* tw = reinterpret_cast<const C*>(a.tw);
     const C* cs = reinterpret_cast<const C*>(a.cs2);
     // raw position of (line l, element e)
@@ -362,6 +355,15 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     // thread -> (line, index): the strided pass runs the line fastest, so that
     // a warp writes row segments; the contiguous pass runs the index fastest
     const Real sc = (Real)(a.out_scale * (a.rhs_scale ? a.dz * a.dz : 1.0));
+    // output strides (computed here, after the FFT, so that they hold no
+    // registers through it): their own (z-tiled spectrum, half spectra) or,
+    // when unset, the input's
+    const bool own = a.o_elem_stride != 0;
+    const long oes = own ? a.o_elem_stride : a.elem_stride;
+    const long ols = own ? a.o_line_stride : a.line_stride;
+    const long ops = own ? a.o_plane_stride : a.plane_stride;
+    const long ots = own ? a.o_tile_stride : a.tile_stride;
+    const long obase = (long)plane * ops + (long)l0 * (ots ? ots : ols);
     auto goff = [&](int l, int e) -> long { return obase + (long)l * ols + (long)e * oes; };
     constexpr int P1 = rp_pitch(N);
     if constexpr (FFTK) {
