@@ -387,7 +387,9 @@ cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool s
         return pp_launch_line_pass(a, inverse, strided, in_cplx, out_cplx, st, true);
     }
     if (lpc > 0) {
-        const int dl = d.kind == PP_KIND_FFT ? lpc : 2 * lpc;
+        // data lines per tile: one per complex FFT line for the full complex
+        // family, two (packed real lines) for the others and the half spectra
+        const int dl = (d.kind == PP_KIND_FFT && !a.half) ? lpc : 2 * lpc;
         a.tw = fp32 ? d.twf.p : d.tw.p;
         a.cs2 = fp32 ? d.csf.p : d.cs.p;
         a.in_cplx = in_cplx;
