@@ -309,7 +309,11 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
                 const T D = X(i);
                 double al, ga;
                 T dn;
-                if (gk != nz - 1) {
+                // with MT rows per lane only the last unrolled row can be the
+                // system's last row: for real spectra the test is resolved at
+                // compile time elsewhere (for complex ones the register cost of
+                // the specialised code outweighs it)
+                if (!((MT == 0 || CPLX || i == MT - 1) && gk == nz - 1)) {
                     const double2 t = tab[i];
                     ga = t.x;
                     al = t.y;
