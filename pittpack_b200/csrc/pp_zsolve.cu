@@ -24,12 +24,12 @@
 //     block's first and last unknown (forward sweep with one division per
 //     row, then a backward sweep), leaving two equations per lane.  Interior
 //     rows have the same coefficients in every block, so the pivots and
-//     spikes of a block depend only on lambda; the group's lane 0 records them
-//     in a shared table that the other lanes read in the backward sweep and
-//     the recovery, so no lane keeps per-row arrays in registers;
-//   * the 2P-row reduced system is solved by parallel cyclic reduction in
-//     shared memory; periodic systems apply Sherman-Morrison to the reduced
-//     system; each lane then recovers its interior rows.
+//     spikes of a block depend only on lambda; the CTA builds them into a
+//     shared table (one reciprocal per entry) that every lane reads;
+//   * eliminating each lane's first unknown leaves a P-row tridiagonal system
+//     in the lanes' last unknowns, solved by parallel cyclic reduction over
+//     warp shuffles (periodic systems through Sherman-Morrison); each lane
+//     then recovers its interior rows.
 #include <type_traits>
 
 #include "pp_common.cuh"
@@ -49,6 +49,23 @@ template <>
 PP_D double zzero<double>() { return 0.0; }
 template <>
 PP_D double2 zzero<double2>() { return make_double2(0.0, 0.0); }
+
+// warp shuffles within segments of w lanes (one lane group)
+PP_D double zshfl(double v, int src, int w) { return __shfl_sync(0xffffffffu, v, src, w); }
+PP_D double2 zshfl(double2 v, int src, int w)
+{
+    return make_double2(__shfl_sync(0xffffffffu, v.x, src, w), __shfl_sync(0xffffffffu, v.y, src, w));
+}
+PP_D double zshfl_up(double v, int d, int w) { return __shfl_up_sync(0xffffffffu, v, d, w); }
+PP_D double2 zshfl_up(double2 v, int d, int w)
+{
+    return make_double2(__shfl_up_sync(0xffffffffu, v.x, d, w), __shfl_up_sync(0xffffffffu, v.y, d, w));
+}
+PP_D double zshfl_down(double v, int d, int w) { return __shfl_down_sync(0xffffffffu, v, d, w); }
+PP_D double2 zshfl_down(double2 v, int d, int w)
+{
+    return make_double2(__shfl_down_sync(0xffffffffu, v.x, d, w), __shfl_down_sync(0xffffffffu, v.y, d, w));
+}
 
 // asynchronous global -> shared copies (LDGSTS): no register staging, every
 // copy of a tile in flight at once
@@ -73,6 +90,58 @@ PP_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"
 PP_HD int zpos(int k) { return k + (k >> 4); }
 PP_HD int zpitch(int nz) { return (zpos(nz - 1) + 1) | 1; }
 
+// Thread order of the tile's load and store (element e of the TS x nz tile ->
+// system s, row k).  Shared memory serves a warp's 8-byte accesses in two
+// phases of 16 threads (16-byte ones in four of 8), so a phase of W threads
+// takes the W / TS rows k0 + r TS (r < W / TS) of its TS systems: with an odd
+// column pitch p the slots s p + k0 + r TS are W distinct banks.  The rows of
+// a phase pair then lie in two 128-byte segments of global memory.
+PP_D int zt_count(int TS, int lts, int nz, int esz)
+{
+    const int W = esz == 16 ? 8 : 16;
+    return TS <= W ? TS * ((nz + W - 1) & ~(W - 1)) : TS * nz;
+}
+PP_D void zt_elem(int e, int TS, int lts, int esz, int* s, int* k)
+{
+    const int lw = esz == 16 ? 3 : 4;
+    const int W = 1 << lw;
+    if (TS > W) {
+        *k = e >> lts;
+        *s = e & (TS - 1);
+        return;
+    }
+    const int blk = e >> (lw + lts);        // W rows of the tile
+    const int f = e & ((W << lts) - 1);
+    const int ph = f >> lw;                 // phase: rows ph + r TS
+    const int jj = f & (W - 1);
+    *s = jj & (TS - 1);
+    *k = (blk << lw) + ph + ((jj >> lts) << lts);
+}
+// f(s, k) for every element of the tile (s < ts, k < nz) in that order.  When
+// the CTA covers whole periods of the order (blockDim.x a multiple of W TS,
+// or of TS where TS > W) each thread keeps its system and steps its row.
+template <typename T, typename F>
+PP_D void zt_each(int TS, int lts, int nz, int ts, F f)
+{
+    const int esz = (int)sizeof(T);
+    const int W = esz == 16 ? 8 : 16;
+    const int period = TS > W ? TS : W * TS;
+    if ((int)blockDim.x >= period) {
+        int s, k;
+        zt_elem(threadIdx.x, TS, lts, esz, &s, &k);
+        const int kst = blockDim.x >> lts;
+        if (s < ts)
+            for (; k < nz; k += kst) f(s, k);
+    } else {
+        const int n = zt_count(TS, lts, nz, esz);
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            int s, k;
+            zt_elem(e, TS, lts, esz, &s, &k);
+            if (s < ts && k < nz) f(s, k);
+        }
+    }
+}
+
 // shared-memory layout of one CTA
 struct ZLayout {
     int pitch;       // tile column pitch (elements)
@@ -95,12 +164,9 @@ PP_HD ZLayout zlayout(int TS, int nz, int P, bool cplx, int nthreads, bool g32 =
     L.tile_off = 0;
     L.tab_off = (size_t)TS * L.pitch * e;
     L.tab_off = (L.tab_off + 15) & ~(size_t)15;
+    // scratch of the pivot-table build: the b_i recurrence of every system
     L.red_off = L.tab_off + (size_t)TS * L.mmax * 16;
-    // per group: 2P rows of a, c, u (doubles) and d (element); before the
-    // sweeps the same bytes hold the b_i recurrence of every system (TS x mmax)
-    const size_t red = (size_t)L.groups * 2 * P * (24 + e);
-    const size_t scr = (size_t)TS * L.mmax * 8;
-    L.bytes = L.red_off + (red > scr ? red : scr);
+    L.bytes = L.red_off + (size_t)TS * L.mmax * 8;
     L.stg_off = (L.bytes + 15) & ~(size_t)15;
     if (g32) L.bytes = L.stg_off + (size_t)TS * nz * (cplx ? 8 : 4);
     return L;
@@ -139,12 +205,6 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
 
     const int group = threadIdx.x / P;
     const int lane = threadIdx.x - group * P;
-    const int m = 2 * P;
-    unsigned char* redb = zsm_raw + Lz.red_off + (size_t)group * m * (24 + sizeof(T));
-    double* ra = reinterpret_cast<double*>(redb);
-    double* rc = ra + m;
-    double* ru = rc + m;
-    T* rd = reinterpret_cast<T*>(ru + m);
 
     const int ky = blockIdx.x / a.tiles_x;
     const int kx0 = (blockIdx.x - ky * a.tiles_x) * a.TS;
@@ -171,12 +231,13 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
                     if (sizeof(T32) == 8) cp_async8(&stg[k * a.TS + s], &g32[k * plane + col0 + s]);
                     else cp_async4(&stg[k * a.TS + s], &g32[k * plane + col0 + s]);
                 }
-            } else {
-                for (int k = threadIdx.x >> lts; k < nz; k += kstep)
-                    if (sizeof(T) == 16) cp_async16(&tile[s * Lz.pitch + zpos(k)], &g[k * plane + col0 + s]);
-                    else cp_async8(&tile[s * Lz.pitch + zpos(k)], &g[k * plane + col0 + s]);
             }
         }
+        if (!G32)
+            zt_each<T>(a.TS, lts, nz, ts, [&](int s2, int k) {
+                if (sizeof(T) == 16) cp_async16(&tile[s2 * Lz.pitch + zpos(k)], &g[k * plane + col0 + s2]);
+                else cp_async8(&tile[s2 * Lz.pitch + zpos(k)], &g[k * plane + col0 + s2]);
+            });
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
     // interior pivots of a block, depending only on lambda: with b_0 = 1,
@@ -219,13 +280,17 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     __syncthreads();
     // Phase 2, every thread: gamma_i = b_{i-1} / b_i, alpha_i = (-1)^{i-1} / b_i,
     // one reciprocal per entry, the entries of all systems spread over the CTA
-    for (int idx = threadIdx.x; idx < ts * mm; idx += blockDim.x) {
-        const int s = idx / mm, i = idx - s * mm;
+    {
+        // blockDim.x / TS threads per system (both powers of two)
+        const int ltp = __ffs(blockDim.x) - 1 - lts;
+        const int s = threadIdx.x >> ltp;
         const double* b = bsc + (size_t)s * mm;
-        if (i == 0 || b[0] == 0.0) continue;
-        const double inv = 1.0 / b[i];
-        reinterpret_cast<double2*>(zsm_raw + Lz.tab_off)[(size_t)s * mm + i] =
-            make_double2(b[i - 1] * inv, (i & 1) ? inv : -inv);
+        if (s < ts && b[0] != 0.0)
+            for (int i = (threadIdx.x & ((1 << ltp) - 1)) + 1; i < mm; i += 1 << ltp) {
+                const double inv = 1.0 / b[i];
+                reinterpret_cast<double2*>(zsm_raw + Lz.tab_off)[(size_t)s * mm + i] =
+                    make_double2(b[i - 1] * inv, (i & 1) ? inv : -inv);
+            }
     }
     cp_async_wait_all();
     __syncthreads();
@@ -260,10 +325,12 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         T* col = tile + (live ? s : 0) * Lz.pitch;
         const double2* tab = reinterpret_cast<const double2*>(zsm_raw + Lz.tab_off) + (size_t)(live ? s : 0) * Lz.mmax;
         // the lane's rows: registers (MT > 0) or the tile column
+        // with MT a power of two >= 8 and s0 = lane MT, zpos(s0 + i) = zpos(s0) + zpos(i)
         T xr[MT > 0 ? MT : 1];
+        T* xcol = col + zpos(s0);
         if constexpr (MT > 0) {
 #pragma unroll
-            for (int i = 0; i < MT; ++i) xr[i] = live ? col[zpos(s0 + i)] : zzero<T>();
+            for (int i = 0; i < MT; ++i) xr[i] = live ? xcol[zpos(i)] : zzero<T>();
         }
         auto X = [&](int i) -> T& {
             if constexpr (MT > 0) return xr[i];
@@ -297,7 +364,10 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             rC0 = C0;
         }
         T rD0 = zzero<T>(), dprev = zzero<T>();
+        // alpha of the block's last row: the table's, or the system's last row
         double aprev = 0.0, gprev = 0.0;
+        bool last_special = false;
+        const double* tg = reinterpret_cast<const double*>(tab);  // gamma_i = tg[2i], alpha_i = tg[2i+1]
         if (live) {
             rD0 = X(0);
             // the tile still holds every lane's input here (registers are
@@ -307,33 +377,34 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             for (int i = 1; i < M; ++i) {
                 const int gk = s0 + i;
                 const T D = X(i);
-                double al, ga;
+                double ga;
                 T dn;
                 // with MT rows per lane only the last unrolled row can be the
                 // system's last row: for real spectra the test is resolved at
                 // compile time elsewhere (for complex ones the register cost of
-                // the specialised code outweighs it)
+                // the specialised code outweighs it).  Interior rows need gamma
+                // only; alpha matters for the block's last row alone.
                 if (!((MT == 0 || CPLX || i == MT - 1) && gk == nz - 1)) {
-                    const double2 t = tab[i];
-                    ga = t.x;
-                    al = t.y;
+                    ga = tg[2 * i];
                     dn = (i == 1) ? zmul(ga, D) : zmul(ga, zsub(D, dprev));
                 } else if (i == 1) {
                     const double inv = 1.0 / BN;
-                    al = AN * inv;
+                    aprev = AN * inv;
                     ga = CN * inv;
                     dn = zmul(inv, D);
+                    last_special = true;
                 } else {
                     const double p = 1.0 / (BN - AN * gprev);
-                    al = -AN * aprev * p;
+                    aprev = -AN * tg[2 * (i - 1) + 1] * p;
                     ga = CN * p;
                     dn = zmul(p, zsub(D, zmul(AN, dprev)));
+                    last_special = true;
                 }
                 X(i) = dn;
-                aprev = al;
                 gprev = ga;
                 dprev = dn;
             }
+            if (!last_special) aprev = tg[2 * (M - 1) + 1];
         }
         // (alpha, gamma, delta) of the block's last row: the reduced row E1
         const double e1a = aprev, e1c = gprev;
@@ -341,20 +412,20 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         __syncwarp(full);
 
         // ---- backward sweep: row 1 in terms of x_0 and x_{M-1} ------------------------
+        // x_1 = dr - br x_0 - cr x_{M-1}.  The spikes are entries of the inverse
+        // of the block's interior matrix tridiag(1, lambda, 1) of order n = M-2:
+        // br = [T^-1]_11 = b_{n-1} / b_n = gamma_n and cr = [T^-1]_1n =
+        // (-1)^{n+1} / b_n = alpha_n, both in the table; only dr is swept.
         double br = 0, cr = 0;
         T dr = zzero<T>();
         if (live && M >= 3) {
             const double2 t2 = tab[M - 2];
-            br = t2.y;
-            cr = t2.x;
+            br = t2.x;
+            cr = t2.y;
             dr = X(M - 2);
+            const double* tg = reinterpret_cast<const double*>(tab);
 #pragma unroll
-            for (int i = M - 3; i >= 1; --i) {
-                const double2 ti = tab[i];
-                dr = zsub(X(i), zmul(ti.x, dr));
-                br = ti.y - ti.x * br;
-                cr = -ti.x * cr;
-            }
+            for (int i = M - 3; i >= 1; --i) dr = zsub(X(i), zmul(tg[2 * i], dr));
         }
         double e0a, e0c;
         T e0d;
@@ -370,88 +441,94 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             e0d = zmul(q, zsub(rD0, zmul(rC0, dr)));
         }
 
-        // ---- reduced system: rows 2L (first) and 2L+1 (last), unit diagonal ---------
-        ra[2 * lane] = e0a;
-        rc[2 * lane] = e0c;
-        rd[2 * lane] = e0d;
-        ru[2 * lane] = 0.0;
-        ra[2 * lane + 1] = e1a;
-        rc[2 * lane + 1] = e1c;
-        rd[2 * lane + 1] = e1d;
-        ru[2 * lane + 1] = 0.0;
-        __syncwarp(full);
-        double beta = 0.0;
-        const double gam = -1.0;
-        if (periodic && lane == 0) {
-            // Sherman-Morrison on the reduced cyclic system: the corners move
-            // into u v^T with u = (gam, 0, .., alpha), v = (1, 0, .., beta / gam)
-            beta = ra[0];
-            const double alpha = rc[m - 1];
-            ra[0] = 0.0;
-            rc[m - 1] = 0.0;
-            const double b0 = 1.0 - gam;
-            rc[0] /= b0;
-            rd[0] = zmul(1.0 / b0, rd[0]);
-            ru[0] = gam / b0;
-            const double bl = 1.0 - alpha * beta / gam;
-            ra[m - 1] /= bl;
-            rd[m - 1] = zmul(1.0 / bl, rd[m - 1]);
-            ru[m - 1] = alpha / bl;
-        }
-        __syncwarp(full);
-        for (int st = 1; st < m; st <<= 1) {
-            double na[2], nc[2], nu[2];
-            T nd[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = 2 * lane + h;
-                const double k1 = ra[r], k2 = rc[r];
-                double a1 = 0, c1 = 0, u1 = 0, a2 = 0, c2 = 0, u2 = 0;
-                T d1 = zzero<T>(), d2 = zzero<T>();
-                if (r - st >= 0) {
-                    a1 = ra[r - st];
-                    c1 = rc[r - st];
-                    u1 = ru[r - st];
-                    d1 = rd[r - st];
-                }
-                if (r + st < m) {
-                    a2 = ra[r + st];
-                    c2 = rc[r + st];
-                    u2 = ru[r + st];
-                    d2 = rd[r + st];
-                }
-                const double inv = 1.0 / (1.0 - k1 * c1 - k2 * a2);
-                na[h] = -k1 * a1 * inv;
-                nc[h] = -k2 * c2 * inv;
-                nu[h] = (ru[r] - k1 * u1 - k2 * u2) * inv;
-                nd[h] = zmul(inv, zsub(zsub(rd[r], zmul(k1, d1)), zmul(k2, d2)));
-            }
-            __syncwarp(full);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = 2 * lane + h;
-                ra[r] = na[h];
-                rc[r] = nc[h];
-                ru[r] = nu[h];
-                rd[r] = nd[h];
-            }
-            __syncwarp(full);
-        }
-        T xf, xl;
-        if (periodic) {
-            // fact = (y_0 + (beta/gam) y_{m-1}) / (1 + z_0 + (beta/gam) z_{m-1})
-            const double b = __shfl_sync(full, beta, threadIdx.x & ~(P - 1) & 31);
-            const double bg = b / gam;
-            const double den = 1.0 + ru[0] + bg * ru[m - 1];
-            const T fact = zmul(1.0 / den, zadd(rd[0], zmul(bg, rd[m - 1])));
-            xf = zsub(rd[2 * lane], zmul(ru[2 * lane], fact));
-            xl = zsub(rd[2 * lane + 1], zmul(ru[2 * lane + 1], fact));
+        // ---- reduced system ---------------------------------------------------------------
+        // lane L's rows E0: f_L + e0a l_{L-1} + e0c l_L = e0d and
+        //                E1: e1a f_L + l_L + e1c f_{L+1} = e1d
+        // in its first (f) and last (l) unknowns.  Eliminating every f_L with E0
+        // leaves a tridiagonal system in l alone, one row per lane (the Schur
+        // complement, diagonally dominant with the original):
+        //   -e1a e0a l_{L-1} + (1 - e1a e0c - e1c e0a') l_L - e1c e0c' l_{L+1}
+        //       = e1d - e1a e0d - e1c e0d'          (' : lane L+1)
+        // The lane indices wrap (periodic z); without it e0a = 0 on the first lane
+        // and e1c = 0 on the last, so the wrapped values carry no weight.  It is
+        // solved by parallel cyclic reduction over warp shuffles, the periodic one
+        // through Sherman-Morrison, and f_L follows from E0.
+        const int nxt = (lane + 1) & (P - 1);
+        const double na0 = zshfl(e0a, nxt, P), nc0 = zshfl(e0c, nxt, P);
+        const T nd0 = zshfl(e0d, nxt, P);
+        double ra = -e1a * e0a;
+        const double rb = 1.0 - e1a * e0c - e1c * na0;
+        double rc = -e1c * nc0;
+        T rd = zsub(zsub(e1d, zmul(e1a, e0d)), zmul(e1c, nd0));
+        T xl;
+        if (P == 1) {
+            // one row: its neighbours on both sides are itself (zero without periodic z)
+            xl = zmul(1.0 / (ra + rb + rc), rd);
         } else {
-            xf = rd[2 * lane];
-            xl = rd[2 * lane + 1];
+            {
+                const double inv = 1.0 / rb;
+                ra *= inv;
+                rc *= inv;
+                rd = zmul(inv, rd);
+            }
+            double ru = 0.0, beta = 0.0;
+            const double gam = -1.0;
+            if (periodic) {
+                // the corners move into u v^T with u = (gam, 0, .., alpha),
+                // v = (1, 0, .., beta / gam): beta = a_0, alpha = c_{P-1}
+                beta = zshfl(ra, 0, P);
+                const double alpha = zshfl(rc, P - 1, P);
+                if (lane == 0) {
+                    const double b0 = 1.0 - gam;
+                    ra = 0.0;
+                    rc /= b0;
+                    rd = zmul(1.0 / b0, rd);
+                    ru = gam / b0;
+                }
+                if (lane == P - 1) {
+                    const double bl = 1.0 - alpha * beta / gam;
+                    rc = 0.0;
+                    ra /= bl;
+                    rd = zmul(1.0 / bl, rd);
+                    ru = alpha / bl;
+                }
+            }
+            for (int st = 1; st < P; st <<= 1) {
+                const bool hp = lane >= st, hn = lane + st < P;
+                double ap = zshfl_up(ra, st, P), cp = zshfl_up(rc, st, P);
+                T dp = zshfl_up(rd, st, P);
+                double an = zshfl_down(ra, st, P), cn = zshfl_down(rc, st, P);
+                T dnx = zshfl_down(rd, st, P);
+                if (!hp) {
+                    ap = cp = 0.0;
+                    dp = zzero<T>();
+                }
+                if (!hn) {
+                    an = cn = 0.0;
+                    dnx = zzero<T>();
+                }
+                const double inv = 1.0 / (1.0 - ra * cp - rc * an);
+                if (periodic) {
+                    const double up = zshfl_up(ru, st, P), un = zshfl_down(ru, st, P);
+                    ru = (ru - ra * (hp ? up : 0.0) - rc * (hn ? un : 0.0)) * inv;
+                }
+                rd = zmul(inv, zsub(zsub(rd, zmul(ra, dp)), zmul(rc, dnx)));
+                ra = -ra * ap * inv;
+                rc = -rc * cn * inv;
+            }
+            if (periodic) {
+                // fact = (y_0 + (beta/gam) y_{P-1}) / (1 + z_0 + (beta/gam) z_{P-1})
+                const double bg = beta / gam;
+                const T y0 = zshfl(rd, 0, P), yl = zshfl(rd, P - 1, P);
+                const double z0 = zshfl(ru, 0, P), zl = zshfl(ru, P - 1, P);
+                const T fact = zmul(1.0 / (1.0 + z0 + bg * zl), zadd(y0, zmul(bg, yl)));
+                xl = zsub(rd, zmul(ru, fact));
+            } else {
+                xl = rd;
+            }
         }
-        __syncwarp(full);
-
+        const T xlp = zshfl(xl, (lane + P - 1) & (P - 1), P);
+        const T xf = zsub(zsub(e0d, zmul(e0a, xlp)), zmul(e0c, xl));
         // ---- recover the block's rows ---------------------------------------------------
         if (live && zero && a.skip_zero) {
             // the kx = ky = 0 column is solved separately (in FP64 from plane sums)
@@ -471,7 +548,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         if constexpr (MT > 0) {
             if (live) {
 #pragma unroll
-                for (int i = 0; i < MT; ++i) col[zpos(s0 + i)] = xr[i];
+                for (int i = 0; i < MT; ++i) xcol[zpos(i)] = xr[i];
             }
         }
         __syncwarp(full);
@@ -485,9 +562,9 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             if (G32)
                 for (int k = threadIdx.x >> lts; k < nz; k += kstep)
                     g32[k * plane + col0 + s] = ZTo32<T>::down(tile[s * Lz.pitch + zpos(k)]);
-            else
-                for (int k = threadIdx.x >> lts; k < nz; k += kstep) g[k * plane + col0 + s] = tile[s * Lz.pitch + zpos(k)];
         }
+        if (!G32)
+            zt_each<T>(a.TS, lts, nz, ts, [&](int s2, int k) { g[k * plane + col0 + s2] = tile[s2 * Lz.pitch + zpos(k)]; });
     }
 }
 
