@@ -91,17 +91,49 @@ constexpr int raw_row_pitch(int elem_bytes)
     return rp;
 }
 
+// The forward DCT-II / DST-II passes read the rows of a strided tile two
+// apart (Makhoul's reorder).  Their raw tile keeps the even rows first and the
+// odd rows from row SPLIT_ODD_BASE on, so that the reads fall on consecutive
+// rows; the base is 4 mod 8 rows so that a row and the next one still land in
+// different banks while the tile is copied in.
+template <int FAM, bool INVERSE, bool STRIDED>
+constexpr bool split_rows() { return STRIDED && !INVERSE && (FAM == F_DCT2 || FAM == F_DST2); }
+template <int N>
+constexpr int split_odd_base() { return (N / 2 + 7 - 4) / 8 * 8 + 4; }
+template <int FAM, bool INVERSE, bool STRIDED, int N>
+constexpr int raw_rows()
+{
+    return split_rows<FAM, INVERSE, STRIDED>() ? split_odd_base<N>() + N / 2 : raw_len<FAM, N>();
+}
+template <int FAM, bool INVERSE, bool STRIDED, int N>
+PP_HD constexpr int raw_row(int e)
+{
+    return split_rows<FAM, INVERSE, STRIDED>() ? ((e & 1) ? split_odd_base<N>() + (e >> 1) : (e >> 1)) : e;
+}
+
+// pitch (complex elements) of an FFT line buffer.  The strided pass reads the
+// lines' spectra four lines by two indices per 8-thread phase: a pitch of
+// 2 mod 8 sixteen-byte units puts them in 8 distinct banks.
+template <int N, bool STRIDED>
+constexpr int line_pitch()
+{
+    if (!STRIDED || N < 64) return rp_pitch(N);
+    int p = rp_pad(N - 1) + 1;
+    while (p % 8 != 2) ++p;
+    return p;
+}
+
 // shared memory of one CTA: the FFT line buffers, or the raw tile that
 // aliases them if that is larger (the padded strided tile)
-template <typename Real, int N, int LPC, int FAM, bool STRIDED>
+template <typename Real, int N, int LPC, int FAM, bool INVERSE, bool STRIDED>
 constexpr size_t smem_bytes()
 {
     using C = typename Vec2<Real>::type;
-    constexpr size_t a1 = (size_t)LPC * rp_pitch(N) * sizeof(C);
+    constexpr size_t a1 = (size_t)LPC * line_pitch<N, STRIDED>() * sizeof(C);
     constexpr size_t a4 = (size_t)2 * LPC * rp_pitch(N / 2) * sizeof(C);
     constexpr size_t lines = a1 > a4 ? a1 : a4;
     constexpr size_t re = raw_cplx<FAM>() ? sizeof(C) : sizeof(Real);
-    constexpr size_t raw = (size_t)raw_len<FAM, N>() *
+    constexpr size_t raw = (size_t)raw_rows<FAM, INVERSE, STRIDED, N>() *
                            (STRIDED ? raw_row_pitch<FAM, LPC>((int)re) : (FAM == F_FFT ? LPC : 2 * LPC)) * re;
     return lines > raw ? lines : raw;
 }
@@ -154,7 +186,9 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     const C* cs = reinterpret_cast<const C*>(a.cs2);
     // raw position of (line l, element e)
     constexpr int RP = raw_row_pitch<FAM, LPC>((int)sizeof(RE));
-    auto ridx = [](int l, int e) -> int { return STRIDED ? e * RP + l : l * LLEN + e; };
+    auto ridx = [](int l, int e) -> int {
+        return STRIDED ? raw_row<FAM, INVERSE, STRIDED, N>(e) * RP + l : l * LLEN + e;
+    };
 
     // ---- 1. load the raw tile ----------------------------------------------------------
     // full tiles whose global element type equals the raw one go in 16-byte
@@ -169,10 +203,17 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
         constexpr int TOT = (STRIDED ? LLEN : DL) * CPR;
         const RE* src = reinterpret_cast<const RE*>(a.src);
         for (int c = tid; c < TOT; c += NT) {
-            const int r = c / CPR;  // run: element row (strided) or line
-            const int k = (c - r * CPR) * PER;
+            int r = c / CPR;  // run: element row (strided) or line
+            int k = (c - r * CPR) * PER;
+            if (STRIDED && CPR == 4 && !split_rows<FAM, INVERSE, STRIDED>()) {
+                // an 8-thread phase copies rows r and r + 4 (odd row pitch in
+                // 16-byte units: 8 distinct banks); a warp still covers 8 rows
+                const int j = c & 31;
+                r = (c >> 5) * 8 + ((j >> 3) & 3) + 4 * ((j >> 2) & 1);
+                k = (j & 3) * PER;
+            }
             const long goff = base + (STRIDED ? (long)r * a.elem_stride : (long)r * a.line_stride) + k;
-            cp_async<16>(raw + r * (STRIDED ? RP : LLEN) + k, src + goff);
+            cp_async<16>(raw + (STRIDED ? raw_row<FAM, INVERSE, STRIDED, N>(r) * RP : r * LLEN) + k, src + goff);
         }
     } else {
         for (int idx = tid; idx < DL * LLEN; idx += NT) {
@@ -244,7 +285,7 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     static_assert(rp_radix(NF, 0) == 8, "the first pass is radix 8");
     const int fl = tid / TPL;           // FFT line of this thread
     const int t = tid - fl * TPL;
-    C* line = sb + fl * (Q4 ? rp_pitch(N / 2) : rp_pitch(N));
+    C* line = sb + fl * (Q4 ? rp_pitch(N / 2) : line_pitch<N, STRIDED>());
     C v[8];
     if constexpr (FFTK) {
 #pragma unroll
@@ -365,7 +406,19 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     const long ots = own ? a.o_tile_stride : a.tile_stride;
     const long obase = (long)plane * ops + (long)l0 * (ots ? ots : ols);
     auto goff = [&](int l, int e) -> long { return obase + (long)l * ols + (long)e * oes; };
-    constexpr int P1 = rp_pitch(N);
+    constexpr int P1 = line_pitch<N, STRIDED>();
+    // the two packed real lines of a strided pass are adjacent in the output:
+    // one 16-byte store for both where the layout allows
+    const bool pair = !a.acc && !a.out_cplx && ols == 1 && ((oes | ops | obase) & 1) == 0 &&
+                      (reinterpret_cast<unsigned long>(a.dst) & 15) == 0;
+    auto put2 = [&](int la, int e, Real va, Real vb) {
+        if (STRIDED && pair && la + 1 < nl) {
+            reinterpret_cast<C*>(reinterpret_cast<Real*>(a.dst) + goff(la, e))[0] = mkc<C>(sc * va, sc * vb);
+        } else {
+            if (la < nl) put<Real>(a, goff(la, e), plane, va, (Real)0, sc);
+            if (la + 1 < nl) put<Real>(a, goff(la + 1, e), plane, vb, (Real)0, sc);
+        }
+    };
     if constexpr (FFTK) {
         for (int idx = tid; idx < LPC * N; idx += NT) {
             int l, e;
@@ -463,7 +516,7 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                 cl = idx >> (LN - 1);
                 kk = idx & (N / 2 - 1);
             }
-            const int la = 2 * cl, lb = la + 1;
+            const int la = 2 * cl;
             const C* ln = sb + cl * P1;
             const int k1 = kk == 0 ? 0 : kk;
             const int k2 = kk == 0 ? N / 2 : N - kk;
@@ -484,8 +537,7 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                     e = N - 1 - k;
                     if (e & 1) sg = (Real)-2;
                 }
-                if (la < nl) put<Real>(a, goff(la, e), plane, sg * (v1x * w.x + v1y * w.y), (Real)0, sc);
-                if (lb < nl) put<Real>(a, goff(lb, e), plane, sg * (v2x * w.x + v2y * w.y), (Real)0, sc);
+                put2(la, e, sg * (v1x * w.x + v1y * w.y), sg * (v2x * w.x + v2y * w.y));
             };
             emit(k1, Z1, P1z, w1);
             emit(k2, Z2, P2z, w2);
@@ -496,14 +548,20 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
         constexpr int LL = rp_log2(LPC);
         for (int idx = tid; idx < LPC * N; idx += NT) {
             int cl, e;
-            if (STRIDED) {
+            if (STRIDED && LPC == 4) {
+                // an 8-thread phase takes outputs e, e + 2 of four lines: their
+                // spectrum slots are adjacent (8 distinct banks)
+                cl = idx & 3;
+                const int rest = idx >> 3;
+                e = 4 * (rest >> 1) + (rest & 1) + 2 * ((idx >> 2) & 1);
+            } else if (STRIDED) {
                 cl = idx & (LPC - 1);
                 e = idx >> LL;
             } else {
                 cl = idx >> LN;
                 e = idx & (N - 1);
             }
-            const int la = 2 * cl, lb = la + 1;
+            const int la = 2 * cl;
             int j = e;
             Real sg = (Real)1;
             if (FAM == F_DST2) {
@@ -511,8 +569,7 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                 if (e & 1) sg = (Real)-1;
             }
             const C z = sb[cl * P1 + rp_pad(mk_pos(j, N))];
-            if (la < nl) put<Real>(a, goff(la, e), plane, sg * z.x, (Real)0, sc);
-            if (lb < nl) put<Real>(a, goff(lb, e), plane, sg * z.y, (Real)0, sc);
+            put2(la, e, sg * z.x, sg * z.y);
         }
     }
 }
@@ -523,7 +580,7 @@ cudaError_t launch_fam(const PPLinePassArgs& a, bool inverse, bool strided, cuda
     dim3 grid(a.nplanes * a.tiles_per_plane), block(LPC * N / 8);
 #define PP_LP2(INV, STR)                                                                                    \
     do {                                                                                                    \
-        constexpr size_t smem = smem_bytes<Real, N, LPC, FAM, STR>();                                       \
+        constexpr size_t smem = smem_bytes<Real, N, LPC, FAM, INV, STR>();                                  \
         auto kfn = lp2_kernel<Real, N, LPC, FAM, INV, STR>;                                                      \
         cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
         if (e != cudaSuccess) return e;                                                                     \
@@ -541,7 +598,7 @@ template <typename Real, int N, int LPC, int FAM>
 cudaError_t launch_half(const PPLinePassArgs& a, cudaStream_t st)
 {
     // the contiguous x pass only: forward real -> half spectra, inverse back
-    constexpr size_t smem = smem_bytes<Real, N, LPC, FAM, false>();
+    constexpr size_t smem = smem_bytes<Real, N, LPC, FAM, FAM == F_C2R, false>();
     auto kfn = lp2_kernel<Real, N, LPC, FAM, FAM == F_C2R, false>;
     cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
