@@ -91,13 +91,19 @@ constexpr int raw_row_pitch(int elem_bytes)
     return rp;
 }
 
-// The forward DCT-II / DST-II passes read the rows of a strided tile two
-// apart (Makhoul's reorder).  Their raw tile keeps the even rows first and the
-// odd rows from row SPLIT_ODD_BASE on, so that the reads fall on consecutive
-// rows; the base is 4 mod 8 rows so that a row and the next one still land in
-// different banks while the tile is copied in.
+// The forward DCT-II / DST-II passes (Makhoul's reorder) and both DCT-IV /
+// DST-IV passes (x[2m], x[N-1-2m]) read the rows of a strided tile two apart.
+// Their raw tile keeps the even rows first and the odd rows from row
+// split_odd_base on, so that the reads fall on consecutive rows; the base is
+// 4 mod 8 rows so that a row and the next one still land in different banks
+// while the tile is copied in.  (The contiguous passes keep their 16-byte
+// copies: an even/odd split there needs 8-byte ones, which cost more than the
+// two-way conflicts they remove.)
 template <int FAM, bool INVERSE, bool STRIDED>
-constexpr bool split_rows() { return STRIDED && !INVERSE && (FAM == F_DCT2 || FAM == F_DST2); }
+constexpr bool split_rows()
+{
+    return STRIDED && ((!INVERSE && (FAM == F_DCT2 || FAM == F_DST2)) || FAM == F_Q4);
+}
 template <int N>
 constexpr int split_odd_base() { return (N / 2 + 7 - 4) / 8 * 8 + 4; }
 template <int FAM, bool INVERSE, bool STRIDED, int N>
