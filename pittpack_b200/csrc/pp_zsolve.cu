@@ -117,27 +117,33 @@ PP_D void zt_elem(int e, int TS, int lts, int esz, int* s, int* k)
     *s = jj & (TS - 1);
     *k = (blk << lw) + ph + ((jj >> lts) << lts);
 }
-// f(s, k) for every element of the tile (s < ts, k < nz) in that order.  When
-// the CTA covers whole periods of the order (blockDim.x a multiple of W TS,
-// or of TS where TS > W) each thread keeps its system and steps its row.
+// f(s, k) for every element of the tile (s < ts, k < nz) in that order.  A
+// thread keeps its system and steps its row: by blockDim.x / TS when the CTA
+// covers whole periods of the order (W TS elements, TS where TS > W); else
+// by blockDim.x / W within a period (R = period / blockDim.x steps) and on
+// to the next period's W rows.  blockDim.x is a power of two >= 32.
 template <typename T, typename F>
 PP_D void zt_each(int TS, int lts, int nz, int ts, F f)
 {
     const int esz = (int)sizeof(T);
     const int W = esz == 16 ? 8 : 16;
     const int period = TS > W ? TS : W * TS;
+    int s, k;
+    zt_elem(threadIdx.x, TS, lts, esz, &s, &k);
+    if (s >= ts) return;
     if ((int)blockDim.x >= period) {
-        int s, k;
-        zt_elem(threadIdx.x, TS, lts, esz, &s, &k);
         const int kst = blockDim.x >> lts;
-        if (s < ts)
-            for (; k < nz; k += kst) f(s, k);
+        for (; k < nz; k += kst) f(s, k);
     } else {
-        const int n = zt_count(TS, lts, nz, esz);
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
-            int s, k;
-            zt_elem(e, TS, lts, esz, &s, &k);
-            if (s < ts && k < nz) f(s, k);
+        const int R = period / blockDim.x, dk = blockDim.x / W;
+        for (int r = 0; k < nz;) {
+            f(s, k);
+            if (++r == R) {
+                r = 0;
+                k += W - (R - 1) * dk;
+            } else {
+                k += dk;
+            }
         }
     }
 }
