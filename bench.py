@@ -63,8 +63,8 @@ KERNEL_NAMES = ["x_forward", "y_forward", "z_solve", "y_inverse", "x_inverse", "
 # DRAM bytes moved / algorithmic bytes per stage, from one ncu capture of the
 # FP64 solve (512 x 512 x 128, NN family; profiles/solve_kernels_dram_traffic_512x512x128.md):
 # reads equal the algorithmic bytes, writes read low by what is still in L2
-DRAM_OVER_ALGORITHMIC = {"x_forward": 14.72 / 16, "y_forward": 14.54 / 16, "z_solve": 14.10 / 16,
-                         "y_inverse": 14.43 / 16, "x_inverse": 22.17 / 24}
+DRAM_OVER_ALGORITHMIC = {"x_forward": 14.62 / 16, "y_forward": 14.69 / 16, "z_solve": 14.11 / 16,
+                         "y_inverse": 14.63 / 16, "x_inverse": 22.15 / 24}
 
 
 LP2_LPC = {16: 16, 32: 16, 64: 8, 128: 8, 256: 4, 512: 4, 1024: 2, 2048: 1}
