@@ -161,24 +161,25 @@ PP_D void rp_butterflies(C* v, int t, const C* __restrict__ tw)
     }
 }
 
-// passes 1..npass-1 (pass 0 is done by the caller-facing entry below)
-template <int SIGN, int N, int P, int NP = rp_npass(N)>
+// passes 1..npass-1 of the power-of-two factor MF of the line length N (pass 0
+// is done by the caller-facing entry below)
+template <int SIGN, int N, int MF, int P, int NP = rp_npass(MF)>
 struct RpRest {
     template <typename C>
     static PP_D void run(C* v, C* line, int t, const C* tw)
     {
-        constexpr int RP = rp_radix(N, P - 1), NSP = rp_ns(N, P - 1);
-        constexpr int R = rp_radix(N, P), NS = rp_ns(N, P);
+        constexpr int RP = rp_radix(MF, P - 1), NSP = rp_ns(MF, P - 1);
+        constexpr int R = rp_radix(MF, P), NS = rp_ns(MF, P);
         __syncthreads();  // everybody finished reading the previous contents
         rp_scatter<N, RP, NSP>(v, line, t);
         __syncthreads();
         rp_gather<N, R>(v, line, t);
         rp_butterflies<SIGN, N, R, NS>(v, t, tw);
-        RpRest<SIGN, N, P + 1, NP>::run(v, line, t, tw);
+        RpRest<SIGN, N, MF, P + 1, NP>::run(v, line, t, tw);
     }
 };
-template <int SIGN, int N, int NP>
-struct RpRest<SIGN, N, NP, NP> {
+template <int SIGN, int N, int MF, int NP>
+struct RpRest<SIGN, N, MF, NP, NP> {
     template <typename C>
     static PP_D void run(C*, C*, int, const C*)
     {
@@ -206,10 +207,15 @@ PP_D int rp_out_index(int t, int j)
 // scratch (contents may still be read by other threads on entry: the first
 // exchange starts with a barrier).  On exit v[j] holds X[rp_out_index(t, j)].
 // Every thread of the block must call it (it contains __syncthreads()).
-template <int SIGN, int N, typename C>
+// MF < N (N = m MF, m odd): only the Stockham passes of the power-of-two
+// factor MF run (spans 1 .. MF/R_last); the caller scatters the last one and
+// finishes with the radix-m pass of span MF.
+template <int SIGN, int N, int MF = N, typename C>
 PP_D void rp_fft(C* v, C* line, int t, const C* __restrict__ tw)
 {
-    static_assert(N >= 8 && (N & (N - 1)) == 0, "power-of-two length >= 8");
-    rp_butterflies<SIGN, N, rp_radix(N, 0), 1>(v, t, tw);
-    RpRest<SIGN, N, 1>::run(v, line, t, tw);
+    static_assert(MF >= 8 && (MF & (MF - 1)) == 0 && N % MF == 0, "power-of-two factor >= 8");
+    rp_butterflies<SIGN, N, rp_radix(MF, 0), 1>(v, t, tw);
+    RpRest<SIGN, N, MF, 1>::run(v, line, t, tw);
 }
+// the largest power of two dividing n
+constexpr int rp_pow2_part(int n) { return n & -n; }

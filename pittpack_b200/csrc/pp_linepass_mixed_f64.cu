@@ -1,0 +1,11 @@
+// FP64 instances of the register-resident transform pass (pp_lp2.cuh) for the
+// lengths 3 2^k and 5 2^k (48 .. 1536): the plain solve.  The power-of-two
+// factor runs as register passes, the odd factor as one shared-memory pass.
+#include "pp_lp2.cuh"
+
+int pp_lpm_lpc(int n) { return pp_lp2::lpm_of(n); }
+
+cudaError_t pp_launch_line_pass_mixed(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
+{
+    return pp_lp2::launch_mixed<double>(a, inverse, strided, st);
+}

@@ -26,6 +26,7 @@
 #include <type_traits>
 
 #include "pp_common.cuh"
+#include "pp_fft.cuh"
 #include "pp_fftreg.cuh"
 #include "pp_kernels.h"
 
@@ -174,7 +175,6 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     constexpr int LLEN = raw_len<FAM, N>();  // raw elements per line
     constexpr int NT = LPC * N / 8;
     constexpr int DL = FFTK ? LPC : 2 * LPC;  // data lines per tile
-    constexpr int LN = rp_log2(N);
     constexpr int LDL = rp_log2(DL);
     // raw tile elements: complex for the FFT family, real otherwise
     using RE = typename std::conditional<RAWC, C, Real>::type;
@@ -231,8 +231,8 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                 l = idx / LLEN;
                 e = idx - l * LLEN;
             } else {
-                l = idx >> LN;
-                e = idx & (N - 1);
+                l = idx / N;
+                e = idx - l * N;
             }
             Real* d = reinterpret_cast<Real*>(raw + ridx(l, e));
             if (l < nl) {
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                            (L.y1 && l0 + nl >= a.ny);
         if (whole) {
             for (int idx = tid; idx < nl * N; idx += NT) {
-                const int l = idx >> LN, e = idx & (N - 1);
+                const int l = idx / N, e = idx - (idx / N) * N;
                 Real* d = reinterpret_cast<Real*>(raw + ridx(l, e));
                 d[0] = d[0] - (Real)(lift_at(L, e, l0 + l, plane, a.nx, a.ny, a.nz) * inv);
             }
@@ -287,8 +287,12 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     // radix 8 first: register q holds point m = t + q N/8 (t < N/8), so the
     // half of the line it falls in is known from q at compile time
     constexpr int NF = Q4 ? N / 2 : N;  // FFT length
+    constexpr int MF = rp_pow2_part(NF);  // its power-of-two factor (register passes)
+    constexpr int MM = NF / MF;           // and its odd factor (one radix-MM pass)
+    static_assert(MM == 1 || MM == 3 || MM == 5, "FFT length 2^k, 3 2^k or 5 2^k");
     constexpr int TPL = NF / 8;         // threads per FFT line
-    static_assert(rp_radix(NF, 0) == 8, "the first pass is radix 8");
+    static_assert(rp_radix(MF, 0) == 8, "the first pass is radix 8");
+    static_assert(!(FAM == F_DST2 && INVERSE) || TPL % 2 == 0, "the DST-III sign uses the parity of t");
     const int fl = tid / TPL;           // FFT line of this thread
     const int t = tid - fl * TPL;
     C* line = sb + fl * (Q4 ? rp_pitch(N / 2) : line_pitch<N, STRIDED>());
@@ -391,11 +395,48 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
 
     // ---- 3. FFT (its first exchange starts with a barrier, so the raw tile
     //         that aliases the line buffers is no longer needed) ----------------------
-    if (INVERSE && !Q4) rp_fft<+1, NF>(v, line, t, tw);
-    else rp_fft<-1, NF>(v, line, t, tw);
+    constexpr int FS = (INVERSE && !Q4) ? +1 : -1;
+    rp_fft<FS, NF, MF>(v, line, t, tw);
     __syncthreads();  // all reads of the last exchange are done
+    if constexpr (MM == 1) {
 #pragma unroll
-    for (int j = 0; j < 8; ++j) line[rp_pad(rp_out_index<NF>(t, j))] = v[j];
+        for (int j = 0; j < 8; ++j) line[rp_pad(rp_out_index<NF>(t, j))] = v[j];
+    } else {
+        // Stockham output of the last register pass, then the final pass of
+        // radix MM and span MF, in place: butterfly j < MF reads points
+        // j + q MF, multiplies point q by W_NF^{q j} and writes output q to
+        // j + q MF (natural order)
+        constexpr int NPM = rp_npass(MF);
+        rp_scatter<NF, rp_radix(MF, NPM - 1), rp_ns(MF, NPM - 1)>(v, line, t);
+        __syncthreads();
+        constexpr int NB = (MF + TPL - 1) / TPL;  // butterflies of this thread, at most
+        C u[NB][MM];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int j = t + b * TPL;
+            if (j < MF) {
+#pragma unroll
+                for (int q = 0; q < MM; ++q) u[b][q] = line[rp_pad(j + q * MF)];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int j = t + b * TPL;
+            if (j < MF) {
+#pragma unroll
+                for (int q = 1; q < MM; ++q) {
+                    C w = __ldg(&tw[q * j]);
+                    if (FS > 0) w.y = -w.y;
+                    u[b][q] = c_mul(u[b][q], w);
+                }
+                if constexpr (MM == 3) dft3<FS>(u[b]);
+                else dft5<FS>(u[b]);
+#pragma unroll
+                for (int q = 0; q < MM; ++q) line[rp_pad(j + q * MF)] = u[b][q];
+            }
+        }
+    }
     __syncthreads();
 
     // ---- 4. post-processing and stores ------------------------------------------------
@@ -432,8 +473,8 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                 l = idx & (LPC - 1);
                 e = idx >> rp_log2(LPC);
             } else {
-                l = idx >> LN;
-                e = idx & (N - 1);
+                l = idx / N;
+                e = idx - l * N;
             }
             if (l >= nl) continue;
             const C z = sb[l * P1 + rp_pad(e)];
@@ -449,8 +490,8 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                 cl = idx & (LPC - 1);
                 kk = idx >> LL;
             } else {
-                cl = idx >> (LN - 1);
-                kk = idx & (N / 2 - 1);
+                cl = idx / (N / 2);
+                kk = idx - cl * (N / 2);
             }
             const int la = 2 * cl, lb = la + 1;
             const C* ln = sb + cl * P1;
@@ -478,8 +519,8 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                 cl = idx & (LPC - 1);
                 e = idx >> LL;
             } else {
-                cl = idx >> LN;
-                e = idx & (N - 1);
+                cl = idx / N;
+                e = idx - cl * N;
             }
             const int la = 2 * cl, lb = la + 1;
             const C z = sb[cl * P1 + rp_pad(e)];
@@ -498,8 +539,8 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                 l = idx & (DL - 1);
                 p = idx >> LDL;
             } else {
-                l = idx >> (LN - 1);
-                p = idx & (NH - 1);
+                l = idx / NH;
+                p = idx - l * NH;
             }
             if (l >= nl) continue;
             const C z = sb[l * P4 + rp_pad(p)];
@@ -519,8 +560,8 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                 cl = idx & (LPC - 1);
                 kk = idx >> LL;
             } else {
-                cl = idx >> (LN - 1);
-                kk = idx & (N / 2 - 1);
+                cl = idx / (N / 2);
+                kk = idx - cl * (N / 2);
             }
             const int la = 2 * cl;
             const C* ln = sb + cl * P1;
@@ -564,8 +605,8 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                 cl = idx & (LPC - 1);
                 e = idx >> LL;
             } else {
-                cl = idx >> LN;
-                e = idx & (N - 1);
+                cl = idx / N;
+                e = idx - cl * N;
             }
             const int la = 2 * cl;
             int j = e;
@@ -616,8 +657,12 @@ template <typename Real, int N, int LPC>
 cudaError_t launch_n(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
 {
     if (a.half && a.kind == PP_KIND_FFT) {
-        if (strided) return cudaErrorInvalidValue;
-        return inverse ? launch_half<Real, N, LPC, F_C2R>(a, st) : launch_half<Real, N, LPC, F_R2C>(a, st);
+        if constexpr ((N & (N - 1)) == 0) {
+            if (strided) return cudaErrorInvalidValue;
+            return inverse ? launch_half<Real, N, LPC, F_C2R>(a, st) : launch_half<Real, N, LPC, F_R2C>(a, st);
+        } else {
+            return cudaErrorInvalidValue;
+        }
     }
     switch (a.kind) {
     case PP_KIND_DST2: return launch_fam<Real, N, LPC, F_DST2>(a, inverse, strided, st);
@@ -656,6 +701,46 @@ cudaError_t launch(const PPLinePassArgs& a, bool inverse, bool strided, cudaStre
     case 512: return launch_n<Real, 512, 4>(a, inverse, strided, st);
     case 1024: return launch_n<Real, 1024, 2>(a, inverse, strided, st);
     case 2048: return launch_n<Real, 2048, 1>(a, inverse, strided, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// lines per CTA for the lengths 3 2^k and 5 2^k of the FP64 kernels (the
+// register passes take the power-of-two factor, one shared-memory pass the
+// odd one); 0 if the length has no such kernel
+inline int lpm_of(int n)
+{
+    switch (n) {
+    case 48: return 8;
+    case 80: return 8;
+    case 96: return 8;
+    case 160: return 4;
+    case 192: return 4;
+    case 320: return 4;
+    case 384: return 4;
+    case 640: return 2;
+    case 768: return 2;
+    case 1280: return 1;
+    case 1536: return 1;
+    default: return 0;
+    }
+}
+
+template <typename Real>
+cudaError_t launch_mixed(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
+{
+    switch (a.n) {
+    case 48: return launch_n<Real, 48, 8>(a, inverse, strided, st);
+    case 80: return launch_n<Real, 80, 8>(a, inverse, strided, st);
+    case 96: return launch_n<Real, 96, 8>(a, inverse, strided, st);
+    case 160: return launch_n<Real, 160, 4>(a, inverse, strided, st);
+    case 192: return launch_n<Real, 192, 4>(a, inverse, strided, st);
+    case 320: return launch_n<Real, 320, 4>(a, inverse, strided, st);
+    case 384: return launch_n<Real, 384, 4>(a, inverse, strided, st);
+    case 640: return launch_n<Real, 640, 2>(a, inverse, strided, st);
+    case 768: return launch_n<Real, 768, 2>(a, inverse, strided, st);
+    case 1280: return launch_n<Real, 1280, 1>(a, inverse, strided, st);
+    case 1536: return launch_n<Real, 1536, 1>(a, inverse, strided, st);
     default: return cudaErrorInvalidValue;
     }
 }
