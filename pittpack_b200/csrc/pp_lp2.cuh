@@ -657,12 +657,8 @@ template <typename Real, int N, int LPC>
 cudaError_t launch_n(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
 {
     if (a.half && a.kind == PP_KIND_FFT) {
-        if constexpr ((N & (N - 1)) == 0) {
-            if (strided) return cudaErrorInvalidValue;
-            return inverse ? launch_half<Real, N, LPC, F_C2R>(a, st) : launch_half<Real, N, LPC, F_R2C>(a, st);
-        } else {
-            return cudaErrorInvalidValue;
-        }
+        if (strided) return cudaErrorInvalidValue;
+        return inverse ? launch_half<Real, N, LPC, F_C2R>(a, st) : launch_half<Real, N, LPC, F_R2C>(a, st);
     }
     switch (a.kind) {
     case PP_KIND_DST2: return launch_fam<Real, N, LPC, F_DST2>(a, inverse, strided, st);

@@ -378,7 +378,7 @@ cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool s
         a.o_tile_stride = a.tile_stride;
     }
     int lpc = pp_lp2_lpc(d.n);
-    const bool mixed = lpc == 0 && !fp32 && !a.half && pp_lpm_lpc(d.n) > 0;
+    const bool mixed = lpc == 0 && !fp32 && pp_lpm_lpc(d.n) > 0;
     if (mixed) lpc = pp_lpm_lpc(d.n);
     if (fp32 && lpc == 0) {
         a.fft = d.fft;
@@ -485,7 +485,8 @@ int z_tile_width(const pp_solver_s* h, bool s_cplx, int ncol, bool fp32)
 // 0 when the path does not apply (the full complex spectrum is used).
 int half_spectrum_cols(const pp_solver_s* h, bool fp32)
 {
-    if (h->tx.kind != PP_KIND_FFT || h->rhs_complex || h->nx < 32 || pp_lp2_lpc(h->nx) == 0) return 0;
+    if (h->tx.kind != PP_KIND_FFT || h->rhs_complex || h->nx < 32) return 0;
+    if (pp_lp2_lpc(h->nx) == 0 && (fp32 || pp_lpm_lpc(h->nx) == 0)) return 0;
     const int lpy = y_lines(h, fp32);
     int q = lpy ? (h->ty.kind == PP_KIND_FFT ? lpy : 2 * lpy) : 1;
     if (q > 16) q = 16;
