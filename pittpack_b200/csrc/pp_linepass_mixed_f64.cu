@@ -1,5 +1,6 @@
 // FP64 instances of the register-resident transform pass (pp_lp2.cuh) for the
-// lengths 3 2^k and 5 2^k (48 .. 1536): the plain solve.  The power-of-two
+// lengths 3 2^k and 5 2^k (48 .. 1536): the plain solve (FP32 instances in
+// pp_linepass_mixed_f32.cu).  The power-of-two
 // factor runs as register passes, the odd factor as one shared-memory pass.
 #include "pp_lp2.cuh"
 

@@ -182,7 +182,7 @@ cudaError_t na_line_pass(PPLinePassArgs a, const NaDir& d, const double2* tw, co
     a.fft = d.fft;
     a.fft.tw = tw;
     a.cs = cs;
-    const int lpc = pp_lp2_lpc(d.n);
+    const int lpc2 = pp_lp2_lpc(d.n), lpc = lpc2 ? lpc2 : pp_lpm_lpc(d.n);
     if (lpc > 0) {
         a.tw = tw;
         a.cs2 = cs;
@@ -191,7 +191,8 @@ cudaError_t na_line_pass(PPLinePassArgs a, const NaDir& d, const double2* tw, co
         const int dl = d.kind == PP_KIND_FFT ? lpc : 2 * lpc;
         a.L = dl;
         a.tiles_per_plane = (a.nlines + dl - 1) / dl;
-        return pp_launch_line_pass_pow2<double, double, double>(a, inverse, strided, st);
+        return lpc2 ? pp_launch_line_pass_pow2<double, double, double>(a, inverse, strided, st)
+                    : pp_launch_line_pass_mixed(a, inverse, strided, st);
     }
     int L = 16;
     while (L > 1 && pp_line_pass_smem(L, d.fft.n) > 64 * 1024) L >>= 1;

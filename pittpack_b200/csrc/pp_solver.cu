@@ -378,7 +378,7 @@ cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool s
         a.o_tile_stride = a.tile_stride;
     }
     int lpc = pp_lp2_lpc(d.n);
-    const bool mixed = lpc == 0 && !fp32 && pp_lpm_lpc(d.n) > 0;
+    const bool mixed = lpc == 0 && pp_lpm_lpc(d.n) > 0;
     if (mixed) lpc = pp_lpm_lpc(d.n);
     if (fp32 && lpc == 0) {
         a.fft = d.fft;
@@ -399,7 +399,9 @@ cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool s
         a.vec16 = runs_aligned16(a, strided, (in_cplx ? 2 : 1) * (fp32 ? sizeof(float) : sizeof(double)), dl);
         a.L = dl;
         a.tiles_per_plane = (a.nlines + dl - 1) / dl;
-        if (mixed) return pp_launch_line_pass_mixed(a, inverse, strided, st);
+        if (mixed)
+            return fp32 ? pp_launch_line_pass_mixed_f32(a, inverse, strided, st)
+                        : pp_launch_line_pass_mixed(a, inverse, strided, st);
         return fp32 ? pp_launch_line_pass_pow2<float, float, float>(a, inverse, strided, st)
                     : pp_launch_line_pass_pow2<double, double, double>(a, inverse, strided, st);
     }
@@ -456,18 +458,18 @@ void set_half_in(PPLinePassArgs& a, int ncol, long splane, int nx, long plane)
 // The forward y pass writes, and the inverse y pass reads, the spectrum as
 // contiguous z tiles (TS adjacent kx x all nz of one ky), so that the z solve
 // moves whole contiguous blocks; TS is the y pass's lines per tile.  Used
-// when the y pass is the register-resident kernel (power-of-two lengths, and
-// 3 2^k / 5 2^k in FP64) with full tiles (nx a multiple of TS), the z solve
-// is the direct one and takes TS systems per CTA.
-int y_lines(const pp_solver_s* h, bool fp32)
+// when the y pass is the register-resident kernel (power-of-two lengths,
+// 3 2^k and 5 2^k) with full tiles (nx a multiple of TS), the z solve is the
+// direct one and takes TS systems per CTA.
+int reg_lines(int n)
 {
-    const int lpc = pp_lp2_lpc(h->ny);
-    return lpc ? lpc : (fp32 ? 0 : pp_lpm_lpc(h->ny));
+    const int lpc = pp_lp2_lpc(n);
+    return lpc ? lpc : pp_lpm_lpc(n);
 }
-int z_tile_width(const pp_solver_s* h, bool s_cplx, int ncol, bool fp32)
+int z_tile_width(const pp_solver_s* h, bool s_cplx, int ncol)
 {
     if (h->opt.z_solver != PP_ZSOLVE_DIRECT) return 0;
-    const int lpc = y_lines(h, fp32);
+    const int lpc = reg_lines(h->ny);
     if (lpc == 0) return 0;
     const int dl = s_cplx ? lpc : 2 * lpc;
     if (dl < 2 || dl > 16 || ncol % dl != 0) return 0;
@@ -483,11 +485,10 @@ int z_tile_width(const pp_solver_s* h, bool s_cplx, int ncol, bool fp32)
 // ~half the columns.  Columns of the spectrum: nx/2 + 1, rounded up to the
 // y pass's lines per tile (<= 16) so that the z-tiled layout still applies;
 // 0 when the path does not apply (the full complex spectrum is used).
-int half_spectrum_cols(const pp_solver_s* h, bool fp32)
+int half_spectrum_cols(const pp_solver_s* h)
 {
-    if (h->tx.kind != PP_KIND_FFT || h->rhs_complex || h->nx < 32) return 0;
-    if (pp_lp2_lpc(h->nx) == 0 && (fp32 || pp_lpm_lpc(h->nx) == 0)) return 0;
-    const int lpy = y_lines(h, fp32);
+    if (h->tx.kind != PP_KIND_FFT || h->rhs_complex || h->nx < 32 || reg_lines(h->nx) == 0) return 0;
+    const int lpy = reg_lines(h->ny);
     int q = lpy ? (h->ty.kind == PP_KIND_FFT ? lpy : 2 * lpy) : 1;
     if (q > 16) q = 16;
     const int c = ((h->nx / 2 + 1 + q - 1) / q) * q;
@@ -511,7 +512,7 @@ int launch_solve(pp_solver_s* h)
     const double dz = -(h->box[4] - h->box[5]) / (nz);
     const long plane = (long)nx * ny;
     // spectrum columns: nx, or the half spectra of the periodic x pass
-    const int hc = half_spectrum_cols(h, false);
+    const int hc = half_spectrum_cols(h);
     const int ncol = hc ? hc : nx;
     const long splane = (long)ncol * ny;
     cudaError_t e;
@@ -562,7 +563,7 @@ int launch_solve(pp_solver_s* h)
     PPLinePassArgs a2 = ay;
     a2.src = h->bufA.as<double>();
     a2.dst = h->bufB.as<double>();
-    const int zt = z_tile_width(h, s_cplx, ncol, false);
+    const int zt = z_tile_width(h, s_cplx, ncol);
     if (zt) set_z_tiled_out(a2, ncol, nz, zt);
     t0 = stamp(h);
     if ((e = line_pass(a2, h->ty, false, true, x_cplx, s_cplx, h->stream)) != cudaSuccess)
@@ -662,7 +663,7 @@ int launch_mixed(pp_solver_s* h)
     const double dy = -(h->box[2] - h->box[3]) / (ny);
     const long plane = (long)nx * ny;
     // spectrum columns: nx, or the half spectra of the periodic x pass
-    const int hc = half_spectrum_cols(h, true);
+    const int hc = half_spectrum_cols(h);
     const int ncol = hc ? hc : nx;
     const long splane = (long)ncol * ny;
     cudaError_t e;
@@ -717,7 +718,7 @@ int launch_mixed(pp_solver_s* h)
     ay.line_stride = 1;
     ay.plane_stride = splane;
 
-    const int zt = z_tile_width(h, s_cplx, ncol, true);
+    const int zt = z_tile_width(h, s_cplx, ncol);
     PPZArgs z{};
     z.data = reinterpret_cast<double*>(B32);
     z.data_fp32 = 1;
@@ -1334,8 +1335,7 @@ int pp_autotune(pp_handle h, int reps, pp_tuning* chosen, double* best_ms)
         }
     }
     // generic transform kernel: lines per tile, only where it runs
-    const bool generic = (pp_lp2_lpc(h->nx) == 0 && pp_lpm_lpc(h->nx) == 0) ||
-                         (pp_lp2_lpc(h->ny) == 0 && pp_lpm_lpc(h->ny) == 0);
+    const bool generic = reg_lines(h->nx) == 0 || reg_lines(h->ny) == 0;
     for (int L = 1; generic && L <= 32 && rc == PP_SUCCESS; L *= 2) {
         pp_tuning t = best;
         t.line_tile = L;

@@ -54,7 +54,8 @@ def test_noalloc_matches_handle_path_on_two_calls():
     L = _lib()
     rng = np.random.default_rng(21)
     cases = [
-        (64, 48, 40, "NNDDDD", (0, 1, 0, 1, 0, 1)),      # mixed-radix y (generic transform kernel)
+        (64, 48, 40, "NNDDDD", (0, 1, 0, 1, 0, 1)),      # 3 2^k y: register passes + radix-3 pass
+        (60, 36, 20, "DDNNDD", (0, 1, 0, 1, 0, 1)),      # lengths of the generic transform kernel
         (128, 64, 32, "PPPPDN", (0, 2, 0, 1, 0.5, 1.5)),  # power-of-two lengths, periodic x/y
     ]
     for nx, ny, nz, bc, box in cases:
