@@ -74,11 +74,15 @@ size_t pp_line_pass_smem(int L, int nfft, bool fp32 = false);
 int pp_lp2_lpc(int n);
 template <typename Real, typename TI, typename TO>
 cudaError_t pp_launch_line_pass_pow2(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st);
-// the same kernel for the lengths 3 2^k (48 .. 1536) and 5 2^k (80 .. 1280):
+// the same kernel for the lengths 3 2^k (48 .. 1536), 5 2^k (80 .. 1280),
+// 9 2^k (144 .. 1152) and 15 2^k (240 .. 960):
 // complex FFT lines per CTA (0 = not covered), and the FP64 / FP32 launches
 int pp_lpm_lpc(int n);
 cudaError_t pp_launch_line_pass_mixed(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st);
 cudaError_t pp_launch_line_pass_mixed_f32(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st);
+// 9 2^k and 15 2^k (144 .. 1152), called by the two above
+cudaError_t pp_launch_line_pass_mixed915(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st);
+cudaError_t pp_launch_line_pass_mixed915_f32(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st);
 // generic 2/3/5-smooth lengths; fp32: the FP32 kernel, twiddles from a.tw and
 // a.cs2 (FP64: a.fft.tw and a.cs), with the refinement epilogue when a.acc is set
 cudaError_t pp_launch_line_pass(const PPLinePassArgs& a, bool inverse, bool strided, bool in_cplx, bool out_cplx,

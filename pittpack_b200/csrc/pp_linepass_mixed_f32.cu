@@ -4,5 +4,6 @@
 
 cudaError_t pp_launch_line_pass_mixed_f32(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
 {
+    if (pp_lp2::lpm_odd9or15(a.n)) return pp_launch_line_pass_mixed915_f32(a, inverse, strided, st);
     return pp_lp2::launch_mixed<float>(a, inverse, strided, st);
 }

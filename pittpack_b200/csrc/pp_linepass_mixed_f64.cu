@@ -8,5 +8,6 @@ int pp_lpm_lpc(int n) { return pp_lp2::lpm_of(n); }
 
 cudaError_t pp_launch_line_pass_mixed(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
 {
+    if (pp_lp2::lpm_odd9or15(a.n)) return pp_launch_line_pass_mixed915(a, inverse, strided, st);
     return pp_lp2::launch_mixed<double>(a, inverse, strided, st);
 }

@@ -56,6 +56,46 @@ struct Vec2<float> {
 
 PP_D int mk_pos(int e, int n) { return (e & 1) ? (n - 1 - (e >> 1)) : (e >> 1); }
 
+// R-point DFT in registers, R = 3 or 5 (pp_fft.cuh)
+template <int SIGN, int R, typename C>
+PP_D void small_dft(C* v)
+{
+    if constexpr (R == 3) dft3<SIGN>(v);
+    else dft5<SIGN>(v);
+}
+
+// MM = A B point DFT by one Cooley-Tukey step: n = B n1 + n2, k = k1 + A k2;
+// A-point DFTs over n1, twiddles W_MM^{n2 k1}, B-point DFTs over n2.  W_MM^x
+// is taken from the FFT's own table as tw[x * stride] (stride = NF / MM).
+template <int SIGN, int A, int B, typename C>
+PP_D void dft_ct(C* v, const C* __restrict__ tw, int stride)
+{
+    C y[B][A];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) {
+#pragma unroll
+        for (int n1 = 0; n1 < A; ++n1) y[n2][n1] = v[B * n1 + n2];
+        small_dft<SIGN, A>(y[n2]);
+    }
+#pragma unroll
+    for (int n2 = 1; n2 < B; ++n2)
+#pragma unroll
+        for (int k1 = 1; k1 < A; ++k1) {
+            C w = __ldg(&tw[n2 * k1 * stride]);
+            if (SIGN > 0) w.y = -w.y;
+            y[n2][k1] = c_mul(y[n2][k1], w);
+        }
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) {
+        C z[B];
+#pragma unroll
+        for (int n2 = 0; n2 < B; ++n2) z[n2] = y[n2][k1];
+        small_dft<SIGN, B>(z);
+#pragma unroll
+        for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = z[k2];
+    }
+}
+
 PP_D double lift_at(const PPLift& L, int i, int j, int k, int nx, int ny, int nz)
 {
     double s = 0.0;
@@ -289,7 +329,7 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     constexpr int NF = Q4 ? N / 2 : N;  // FFT length
     constexpr int MF = rp_pow2_part(NF);  // its power-of-two factor (register passes)
     constexpr int MM = NF / MF;           // and its odd factor (one radix-MM pass)
-    static_assert(MM == 1 || MM == 3 || MM == 5, "FFT length 2^k, 3 2^k or 5 2^k");
+    static_assert(MM == 1 || MM == 3 || MM == 5 || MM == 9 || MM == 15, "FFT length 2^k, 3 2^k, 5 2^k, 9 2^k or 15 2^k");
     constexpr int TPL = NF / 8;         // threads per FFT line
     static_assert(rp_radix(MF, 0) == 8, "the first pass is radix 8");
     static_assert(!(FAM == F_DST2 && INVERSE) || TPL % 2 == 0, "the DST-III sign uses the parity of t");
@@ -430,8 +470,9 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
                     if (FS > 0) w.y = -w.y;
                     u[b][q] = c_mul(u[b][q], w);
                 }
-                if constexpr (MM == 3) dft3<FS>(u[b]);
-                else dft5<FS>(u[b]);
+                if constexpr (MM == 3 || MM == 5) small_dft<FS, MM>(u[b]);
+                else if constexpr (MM == 9) dft_ct<FS, 3, 3>(u[b], tw, MF);
+                else dft_ct<FS, 5, 3>(u[b], tw, MF);
 #pragma unroll
                 for (int q = 0; q < MM; ++q) line[rp_pad(j + q * MF)] = u[b][q];
             }
@@ -701,24 +742,49 @@ cudaError_t launch(const PPLinePassArgs& a, bool inverse, bool strided, cudaStre
     }
 }
 
-// lines per CTA for the lengths 3 2^k and 5 2^k of the FP64 kernels (the
-// register passes take the power-of-two factor, one shared-memory pass the
-// odd one); 0 if the length has no such kernel
+// lines per CTA for the lengths m 2^k, m = 3, 5, 9, 15, with 2^k >= 16 so
+// that the quarter-wave families' half-length FFT still starts with a
+// radix-8 register pass (the register passes take the power-of-two factor,
+// one shared-memory pass the odd one); 0 if the length has no such kernel
 inline int lpm_of(int n)
 {
     switch (n) {
     case 48: return 8;
     case 80: return 8;
     case 96: return 8;
+    case 144: return 8;
     case 160: return 4;
     case 192: return 4;
+    case 240: return 4;
+    case 288: return 4;
     case 320: return 4;
     case 384: return 4;
+    case 480: return 2;
+    case 576: return 2;
     case 640: return 2;
     case 768: return 2;
+    case 960: return 1;
+    case 1152: return 1;
     case 1280: return 1;
     case 1536: return 1;
     default: return 0;
+    }
+}
+inline bool lpm_odd9or15(int n) { return n == 144 || n == 240 || n == 288 || n == 480 || n == 576 || n == 960 || n == 1152; }
+
+// the odd factors 9 and 15 (their own translation units)
+template <typename Real>
+cudaError_t launch_mixed915(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
+{
+    switch (a.n) {
+    case 144: return launch_n<Real, 144, 8>(a, inverse, strided, st);
+    case 240: return launch_n<Real, 240, 4>(a, inverse, strided, st);
+    case 288: return launch_n<Real, 288, 4>(a, inverse, strided, st);
+    case 480: return launch_n<Real, 480, 2>(a, inverse, strided, st);
+    case 576: return launch_n<Real, 576, 2>(a, inverse, strided, st);
+    case 960: return launch_n<Real, 960, 1>(a, inverse, strided, st);
+    case 1152: return launch_n<Real, 1152, 1>(a, inverse, strided, st);
+    default: return cudaErrorInvalidValue;
     }
 }
 

@@ -96,11 +96,6 @@ PP_HD int zpitch(int nz) { return (zpos(nz - 1) + 1) | 1; }
 // takes the W / TS rows k0 + r TS (r < W / TS) of its TS systems: with an odd
 // column pitch p the slots s p + k0 + r TS are W distinct banks.  The rows of
 // a phase pair then lie in two 128-byte segments of global memory.
-PP_D int zt_count(int TS, int lts, int nz, int esz)
-{
-    const int W = esz == 16 ? 8 : 16;
-    return TS <= W ? TS * ((nz + W - 1) & ~(W - 1)) : TS * nz;
-}
 PP_D void zt_elem(int e, int TS, int lts, int esz, int* s, int* k)
 {
     const int lw = esz == 16 ? 3 : 4;
@@ -231,11 +226,19 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         if (s < ts) {
             if (G32) {
                 // FP32 elements copied asynchronously into the staging area;
-                // converted to the FP64 tile once they have landed
+                // converted to the FP64 tile once they have landed.  A full
+                // z tile is one contiguous block: 16-byte chunks
                 T32* stg = reinterpret_cast<T32*>(zsm_raw + Lz.stg_off);
-                for (int k = threadIdx.x >> lts; k < nz; k += kstep) {
-                    if (sizeof(T32) == 8) cp_async8(&stg[k * a.TS + s], &g32[k * plane + col0 + s]);
-                    else cp_async4(&stg[k * a.TS + s], &g32[k * plane + col0 + s]);
+                const int tbytes = nz * a.TS * (int)sizeof(T32);
+                if (a.tiled && ts == a.TS && tbytes % 16 == 0) {
+                    const char* src = reinterpret_cast<const char*>(g32 + col0);
+                    for (int c = threadIdx.x; c < tbytes / 16; c += blockDim.x)
+                        cp_async16(reinterpret_cast<char*>(stg) + 16 * c, src + 16 * c);
+                } else {
+                    for (int k = threadIdx.x >> lts; k < nz; k += kstep) {
+                        if (sizeof(T32) == 8) cp_async8(&stg[k * a.TS + s], &g32[k * plane + col0 + s]);
+                        else cp_async4(&stg[k * a.TS + s], &g32[k * plane + col0 + s]);
+                    }
                 }
             }
         }
@@ -302,11 +305,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     __syncthreads();
     if (G32) {
         const T32* stg = reinterpret_cast<const T32*>(zsm_raw + Lz.stg_off);
-        const int s = threadIdx.x & (a.TS - 1);
-        const int kstep = blockDim.x >> lts;
-        if (s < ts)
-            for (int k = threadIdx.x >> lts; k < nz; k += kstep)
-                tile[s * Lz.pitch + zpos(k)] = ZTo32<T>::up(stg[k * a.TS + s]);
+        zt_each<T>(a.TS, lts, nz, ts, [&](int s2, int k) { tile[s2 * Lz.pitch + zpos(k)] = ZTo32<T>::up(stg[k * a.TS + s2]); });
         __syncthreads();
     }
 
@@ -561,17 +560,12 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     }
     __syncthreads();
 
-    {
-        const int s = threadIdx.x & (a.TS - 1);
-        const int kstep = blockDim.x >> lts;
-        if (s < ts) {
-            if (G32)
-                for (int k = threadIdx.x >> lts; k < nz; k += kstep)
-                    g32[k * plane + col0 + s] = ZTo32<T>::down(tile[s * Lz.pitch + zpos(k)]);
-        }
-        if (!G32)
-            zt_each<T>(a.TS, lts, nz, ts, [&](int s2, int k) { g[k * plane + col0 + s2] = tile[s2 * Lz.pitch + zpos(k)]; });
-    }
+    if (G32)
+        zt_each<T>(a.TS, lts, nz, ts, [&](int s2, int k) {
+            g32[k * plane + col0 + s2] = ZTo32<T>::down(tile[s2 * Lz.pitch + zpos(k)]);
+        });
+    else
+        zt_each<T>(a.TS, lts, nz, ts, [&](int s2, int k) { g[k * plane + col0 + s2] = tile[s2 * Lz.pitch + zpos(k)]; });
 }
 
 }  // namespace

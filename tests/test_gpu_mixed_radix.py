@@ -1,6 +1,7 @@
-"""Parity of the register-resident transform pass for the lengths 3 2^k and
-5 2^k (48 .. 1536): its power-of-two factor runs as register passes, the odd
-factor as one shared-memory radix-3/5 pass.  Every such length in x
+"""Parity of the register-resident transform pass for the lengths m 2^k,
+m = 3, 5, 9, 15 (48 .. 1536): its power-of-two factor runs as register
+passes, the odd factor as one shared-memory pass (radix 3 or 5, or a
+Cooley-Tukey DFT-9 = 3 x 3 or DFT-15 = 5 x 3).  Every such length in x
 (contiguous pass) and in y (strided pass, z-tiled spectrum), for the real,
 periodic and quarter-wave families, against the CPU oracle at the plain
 path's bar (relative L2 <= 1e-12)."""
@@ -12,7 +13,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
-LENGTHS = [48, 80, 96, 160, 192, 320, 384, 640, 768, 1280, 1536]
+LENGTHS = [48, 80, 96, 144, 160, 192, 240, 288, 320, 384, 480, 576, 640, 768, 960, 1152, 1280, 1536]
 FAMS = ["NNNNDD", "DDDDDD", "PPPPDD", "NDNDNN", "DNDNPP", "NNDDDN"]
 
 
