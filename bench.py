@@ -67,7 +67,11 @@ DRAM_OVER_ALGORITHMIC = {"x_forward": 14.62 / 16, "y_forward": 14.69 / 16, "z_so
                          "y_inverse": 14.63 / 16, "x_inverse": 22.15 / 24}
 
 
-LP2_LPC = {16: 16, 32: 16, 64: 8, 128: 8, 256: 4, 512: 4, 1024: 2, 2048: 1}
+# complex FFT lines per CTA of the register-resident transform kernel, by
+# length (powers of two, and m 2^k for m = 3, 5, 9, 15), as the library uses
+LP2_LPC = {16: 16, 32: 16, 64: 8, 128: 8, 256: 4, 512: 4, 1024: 2, 2048: 1,
+           48: 8, 80: 8, 96: 8, 144: 8, 160: 4, 192: 4, 240: 4, 288: 4, 320: 4, 384: 4,
+           480: 2, 576: 2, 640: 2, 768: 2, 960: 1, 1152: 1, 1280: 1, 1536: 1}
 
 
 def half_cols(n: int, bc: str, rhs_complex: bool = False, ny: int = 0) -> float:

@@ -283,10 +283,9 @@ extern "C" int pp_solve_noalloc(int nx, int ny, int nz, const char bc[6], const 
     if (!cv.ok) return PP_NOALLOC_TOO_LARGE;
 
     cudaStream_t st = (cudaStream_t)stream;
-    cudaError_t e;
-#define PP_NA_UP(dst, vec)                                                                                      \
-    if ((e = cudaMemcpyAsync(dst, (vec).data(), sizeof((vec)[0]) * (vec).size(), cudaMemcpyHostToDevice, st)) != \
-        cudaSuccess)                                                                                            \
+#define PP_NA_UP(dst, vec)                                                                                     \
+    if (cudaMemcpyAsync(dst, (vec).data(), sizeof((vec)[0]) * (vec).size(), cudaMemcpyHostToDevice, st) !=      \
+        cudaSuccess)                                                                                           \
         return PP_CUDA_ERROR;
     PP_NA_UP(twx, tx.tw);
     PP_NA_UP(csx, tx.cs);

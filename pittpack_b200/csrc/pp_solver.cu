@@ -883,11 +883,14 @@ int pp_create(int nx, int ny, int nz, pp_handle* out)
     cudaGetDevice(&h->device);
     pp_default_options(&h->opt);
     const size_t n = (size_t)nx * ny * nz;
-    cudaError_t e;
-    if ((e = h->rhs.alloc(2 * n * sizeof(double))) != cudaSuccess ||
-        (e = h->bufA.alloc(2 * n * sizeof(double))) != cudaSuccess ||
-        (e = h->bufB.alloc(2 * n * sizeof(double))) != cudaSuccess ||
-        (e = h->out.alloc(2 * n * sizeof(double))) != cudaSuccess) {
+    if (h->rhs.alloc(2 * n * sizeof(double)) != cudaSuccess || h->bufA.alloc(2 * n * sizeof(double)) != cudaSuccess ||
+        h->bufB.alloc(2 * n * sizeof(double)) != cudaSuccess || h->out.alloc(2 * n * sizeof(double)) != cudaSuccess) {
+        // release what did fit (the buffers have no destructor)
+        h->rhs.free();
+        h->bufA.free();
+        h->bufB.free();
+        h->out.free();
+        cudaGetLastError();
         delete h;
         return PP_ALLOCATION_FAIL;
     }
