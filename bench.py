@@ -369,6 +369,16 @@ def run_serve_leg(args):
                                            sweeps=args.sweeps))
                 if st != 0:
                     raise RuntimeError(f"warm-up request {n}^3 {bc} failed with status {st}")
+        # and the whole stream once back to back (10 outstanding), so that the
+        # pool also holds the second handles of shapes that overlap in flight
+        wt = []
+        for i, (n, bc) in enumerate(reqs):
+            if i >= len(ring):
+                S.wait(wt[i - len(ring)])
+            wt.append(S.submit(n, n, n, bc, rhs[:n ** 3], ring[i % len(ring)][:n ** 3], precision=prec,
+                               sweeps=args.sweeps))
+        for t in wt[max(0, count - len(ring)):]:
+            S.wait(t)
         per_rate = []
         for rate in SERVE_RATES:
             arr = np.cumsum(np.random.default_rng(11 + rate).exponential(1.0 / rate, count))
