@@ -109,12 +109,16 @@ struct PPZArgs {
 };
 
 // lanes that share one z system (a power of two <= 32)
-int pp_zsolve_lanes(int nz, bool cplx);
+int pp_zsolve_lanes(int nz, bool cplx, bool large = false);
+// grids of at least this many z systems (kx x ky columns) keep uneven row
+// counts in registers too (the register capacity path of the z solve)
+#define PP_Z_LARGE_SYSTEMS 65536L
+bool pp_zsolve_large(long systems);
 // systems per CTA and threads per CTA of the z solve
 void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads);
 // the same for a chosen lane count (0 or invalid: the default); the launch
 // must then carry P = that lane count
-void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* threads, int systems = 0);
+void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* threads, int systems = 0, int ny = 0);
 int pp_zsolve_valid_lanes(int nz, int P);
 size_t pp_zsolve_smem_p(int TS, int nz, bool cplx, int P);
 

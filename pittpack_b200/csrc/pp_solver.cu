@@ -475,7 +475,7 @@ int z_tile_width(const pp_solver_s* h, bool s_cplx, int ncol)
     if (dl < 2 || dl > 16 || ncol % dl != 0) return 0;
     if (h->tune.zsolve_tile != 0 && h->tune.zsolve_tile != dl) return 0;
     int ts = 0, threads = 0;
-    pp_zsolve_config_p(h->nz, s_cplx, ncol, h->tune.zsolve_lanes, &ts, &threads, dl);
+    pp_zsolve_config_p(h->nz, s_cplx, ncol, h->tune.zsolve_lanes, &ts, &threads, dl, h->ny);
     return ts == dl ? dl : 0;
 }
 
@@ -576,7 +576,7 @@ int launch_solve(pp_solver_s* h)
     z.ny = ny;
     z.nz = nz;
     int zthreads = 0;
-    pp_zsolve_config_p(nz, s_cplx, ncol, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile);
+    pp_zsolve_config_p(nz, s_cplx, ncol, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile, ny);
     z.P = h->tune.zsolve_lanes;
     z.tiled = zt ? 1 : 0;
     z.tiles_x = (ncol + z.TS - 1) / z.TS;
@@ -727,7 +727,7 @@ int launch_mixed(pp_solver_s* h)
     z.ny = ny;
     z.nz = nz;
     int zthreads = 0;
-    pp_zsolve_config_p(nz, s_cplx, ncol, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile);
+    pp_zsolve_config_p(nz, s_cplx, ncol, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile, ny);
     z.P = h->tune.zsolve_lanes;
     z.tiled = zt ? 1 : 0;
     z.tiles_x = (ncol + z.TS - 1) / z.TS;

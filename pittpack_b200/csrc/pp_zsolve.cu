@@ -96,11 +96,6 @@ PP_HD int zpitch(int nz) { return (zpos(nz - 1) + 1) | 1; }
 // takes the W / TS rows k0 + r TS (r < W / TS) of its TS systems: with an odd
 // column pitch p the slots s p + k0 + r TS are W distinct banks.  The rows of
 // a phase pair then lie in two 128-byte segments of global memory.
-PP_D int zt_count(int TS, int lts, int nz, int esz)
-{
-    const int W = esz == 16 ? 8 : 16;
-    return TS <= W ? TS * ((nz + W - 1) & ~(W - 1)) : TS * nz;
-}
 PP_D void zt_elem(int e, int TS, int lts, int esz, int* s, int* k)
 {
     const int lw = esz == 16 ? 3 : 4;
@@ -194,11 +189,13 @@ struct ZTo32<double2> {
 };
 
 // G32: the spectrum in global memory is FP32 (refined mixed-precision solve);
-// the tile and all arithmetic stay FP64.  MT > 0: every lane owns exactly MT
-// rows (nz = P MT) and keeps them in registers through the three sweeps,
-// reading and writing its rows of the tile once; MT = 0: any nz, the sweeps
-// work on the tile in shared memory.
-template <bool CPLX, bool G32, int MT>
+// the tile and all arithmetic stay FP64.  MT > 0: every lane keeps its rows
+// in registers through the three sweeps, reading and writing its rows of the
+// tile once -- exactly MT rows each (CAP = false, nz = P MT, MT = 8, 16, 32),
+// or at most MT (CAP = true, MT = 8, 12, 16, 24, 32: M = nz / P or one more,
+// the registers indexed statically under i < M guards); MT = 0: any nz, the
+// sweeps work on the tile in shared memory.
+template <bool CPLX, bool G32, int MT, bool CAP>
 __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
 {
     using T = typename std::conditional<CPLX, double2, double>::type;
@@ -312,7 +309,8 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
 
     const int bsz = nz / P;
     const int rem = nz - bsz * P;
-    const int M = MT > 0 ? MT : bsz + (lane < rem ? 1 : 0);
+    constexpr bool EXACT = MT > 0 && !CAP;
+    const int M = EXACT ? MT : bsz + (lane < rem ? 1 : 0);
     const int s0 = lane * bsz + min(lane, rem);
     const bool periodic = a.zlo == PP_Z_PERIODIC;
     const bool has_d = a.zlo == PP_Z_DIRICHLET || a.zhi == PP_Z_DIRICHLET;
@@ -334,9 +332,12 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         // with MT a power of two >= 8 and s0 = lane MT, zpos(s0 + i) = zpos(s0) + zpos(i)
         T xr[MT > 0 ? MT : 1];
         T* xcol = col + zpos(s0);
-        if constexpr (MT > 0) {
+        if constexpr (EXACT) {
 #pragma unroll
             for (int i = 0; i < MT; ++i) xr[i] = live ? xcol[zpos(i)] : zzero<T>();
+        } else if constexpr (MT > 0) {
+#pragma unroll
+            for (int i = 0; i < MT; ++i) xr[i] = (live && i < M) ? col[zpos(s0 + i)] : zzero<T>();
         }
         auto X = [&](int i) -> T& {
             if constexpr (MT > 0) return xr[i];
@@ -380,7 +381,8 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             // written back at the end)
             if (s0 == 0 && periodic && pin) rD0 = zmul(0.5, zadd(rD0, col[zpos(nz - 1)]));
 #pragma unroll
-            for (int i = 1; i < M; ++i) {
+            for (int i = 1; i < (MT > 0 ? MT : M); ++i) {
+                if (CAP && i >= M) break;
                 const int gk = s0 + i;
                 const T D = X(i);
                 double ga;
@@ -390,7 +392,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
                 // compile time elsewhere (for complex ones the register cost of
                 // the specialised code outweighs it).  Interior rows need gamma
                 // only; alpha matters for the block's last row alone.
-                if (!((MT == 0 || CPLX || i == MT - 1) && gk == nz - 1)) {
+                if (!((MT == 0 || CAP || CPLX || i == MT - 1) && gk == nz - 1)) {
                     ga = tg[2 * i];
                     dn = (i == 1) ? zmul(ga, D) : zmul(ga, zsub(D, dprev));
                 } else if (i == 1) {
@@ -428,10 +430,19 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             const double2 t2 = tab[M - 2];
             br = t2.x;
             cr = t2.y;
-            dr = X(M - 2);
             const double* tg = reinterpret_cast<const double*>(tab);
+            if constexpr (CAP) {
+                // registers indexed statically: rows above M - 2 are skipped
 #pragma unroll
-            for (int i = M - 3; i >= 1; --i) dr = zsub(X(i), zmul(tg[2 * i], dr));
+                for (int i = MT - 2; i >= 1; --i) {
+                    if (i > M - 2) continue;
+                    dr = (i == M - 2) ? X(i) : zsub(X(i), zmul(tg[2 * i], dr));
+                }
+            } else {
+                dr = X(M - 2);
+#pragma unroll
+                for (int i = M - 3; i >= 1; --i) dr = zsub(X(i), zmul(tg[2 * i], dr));
+            }
         }
         double e0a, e0c;
         T e0d;
@@ -539,7 +550,21 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         if (live && zero && a.skip_zero) {
             // the kx = ky = 0 column is solved separately (in FP64 from plane sums)
 #pragma unroll
-            for (int i = 0; i < M; ++i) X(i) = zzero<T>();
+            for (int i = 0; i < (MT > 0 ? MT : M); ++i) X(i) = zzero<T>();
+        } else if (live && CAP) {
+            T xn = xl;
+#pragma unroll
+            for (int i = MT - 1; i >= 1; --i) {
+                if (i > M - 1) continue;
+                if (i == M - 1) {
+                    X(i) = xl;
+                } else {
+                    const double2 ti = tab[i];
+                    xn = zsub(zsub(X(i), zmul(ti.y, xf)), zmul(ti.x, xn));
+                    X(i) = xn;
+                }
+            }
+            X(0) = xf;
         } else if (live) {
             T xn = xl;
             X(M - 1) = xl;
@@ -551,47 +576,59 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             }
             X(0) = xf;
         }
-        if constexpr (MT > 0) {
+        if constexpr (EXACT) {
             if (live) {
 #pragma unroll
                 for (int i = 0; i < MT; ++i) xcol[zpos(i)] = xr[i];
+            }
+        } else if constexpr (MT > 0) {
+            if (live) {
+#pragma unroll
+                for (int i = 0; i < MT; ++i)
+                    if (i < M) col[zpos(s0 + i)] = xr[i];
             }
         }
         __syncwarp(full);
     }
     __syncthreads();
 
-    {
+    if (G32) {
         const int s = threadIdx.x & (a.TS - 1);
         const int kstep = blockDim.x >> lts;
-        if (s < ts) {
-            if (G32)
-                for (int k = threadIdx.x >> lts; k < nz; k += kstep)
-                    g32[k * plane + col0 + s] = ZTo32<T>::down(tile[s * Lz.pitch + zpos(k)]);
-        }
-        if (!G32)
-            zt_each<T>(a.TS, lts, nz, ts, [&](int s2, int k) { g[k * plane + col0 + s2] = tile[s2 * Lz.pitch + zpos(k)]; });
-    }
+        if (s < ts)
+            for (int k = threadIdx.x >> lts; k < nz; k += kstep)
+                g32[k * plane + col0 + s] = ZTo32<T>::down(tile[s * Lz.pitch + zpos(k)]);
+    } else
+        zt_each<T>(a.TS, lts, nz, ts, [&](int s2, int k) { g[k * plane + col0 + s2] = tile[s2 * Lz.pitch + zpos(k)]; });
 }
 
 }  // namespace
 
-int pp_zsolve_lanes(int nz, bool cplx)
+int pp_zsolve_lanes(int nz, bool cplx, bool large)
 {
     // about 32 rows per lane (16 for complex data, whose tile is twice as
-    // large, so that a CTA still keeps every group busy)
+    // large, so that a CTA still keeps every group busy).  Grids with many
+    // systems (large) take the fewest lanes that leave at most that many rows,
+    // so that any nz keeps its rows in registers; smaller grids keep more
+    // resident CTAs with the shared-memory rows (batches of small grids run
+    // concurrently, where occupancy counts more)
     const int rows = cplx ? 16 : 32;
     int P = 1;
-    while (P < 32 && 2 * P <= nz / rows) P *= 2;
+    if (large)
+        while (P < 32 && (nz + P - 1) / P > rows) P *= 2;
+    else
+        while (P < 32 && 2 * P <= nz / rows) P *= 2;
     while (P > 1 && P > nz / 2) P /= 2;
     return P;
 }
+
+bool pp_zsolve_large(long systems) { return systems >= PP_Z_LARGE_SYSTEMS; }
 
 // launch shape: systems per CTA (one lane group each) and threads per CTA,
 // keeping the CTA within ~56 KB of shared memory so about four fit on an SM
 void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads)
 {
-    const int P = pp_zsolve_lanes(nz, cplx);
+    const int P = pp_zsolve_lanes(nz, cplx, false);
     int ts = PP_Z_THREADS / P;
     auto bytes = [&](int t) {
         const int th = t * P < 32 ? 32 : t * P;
@@ -605,7 +642,7 @@ void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads)
 
 size_t pp_zsolve_smem(int TS, int nz, bool cplx)
 {
-    return pp_zsolve_smem_p(TS, nz, cplx, pp_zsolve_lanes(nz, cplx));
+    return pp_zsolve_smem_p(TS, nz, cplx, pp_zsolve_lanes(nz, cplx, false));
 }
 
 // a lane count the kernel accepts: a power of two <= 32 leaving every lane at
@@ -623,9 +660,9 @@ size_t pp_zsolve_smem_p(int TS, int nz, bool cplx, int P)
 
 // the launch shape for a chosen lane count (0 or invalid: the default) and
 // systems per CTA (0: as many as fit ~56 KB of shared memory)
-void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* threads, int systems)
+void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* threads, int systems, int ny)
 {
-    const int P = pp_zsolve_valid_lanes(nz, lanes) ? lanes : pp_zsolve_lanes(nz, cplx);
+    const int P = pp_zsolve_valid_lanes(nz, lanes) ? lanes : pp_zsolve_lanes(nz, cplx, pp_zsolve_large((long)nx * ny));
     int ts = PP_Z_THREADS / P;
     if (systems >= 1 && (systems & (systems - 1)) == 0 && systems <= ts) {
         ts = systems;
@@ -641,29 +678,41 @@ cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
 {
     if (a0.nz < 3 || a0.nz > PP_Z_MAX_NZ) return cudaErrorInvalidValue;
     PPZArgs a = a0;
-    if (!pp_zsolve_valid_lanes(a.nz, a.P)) a.P = pp_zsolve_lanes(a.nz, cplx);
+    const bool large = pp_zsolve_large((long)a.nx * a.ny);
+    if (!pp_zsolve_valid_lanes(a.nz, a.P)) a.P = pp_zsolve_lanes(a.nz, cplx, large);
     const int threads = a.TS * a.P < 32 ? 32 : a.TS * a.P;
     if (threads > PP_Z_THREADS) return cudaErrorInvalidValue;
     const size_t smem = zlayout(a.TS, a.nz, a.P, cplx, threads, a.data_fp32 != 0).bytes;
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     dim3 grid(a.ny * a.tiles_x), block(threads);
     cudaError_t e;
-    // rows per lane fixed at compile time where every lane has the same count
-    const int rows = a.nz / a.P;
+    // rows per lane fixed at compile time where every lane has the same count;
+    // else the smallest register capacity that holds every lane's rows
+    const int rows = a.nz / a.P, rmax = (a.nz + a.P - 1) / a.P;
     const int mt = (a.nz % a.P == 0 && (rows == 8 || rows == 16 || (rows == 32 && !cplx))) ? rows : 0;
-#define PP_ZL(C, G, M)                                                                                          \
+    int cap = 0;
+    if (!mt && large) {
+        if (cplx) cap = rmax <= 8 ? 8 : rmax <= 12 ? 12 : rmax <= 16 ? 16 : 0;
+        else cap = rmax <= 8 ? 8 : rmax <= 16 ? 16 : rmax <= 24 ? 24 : rmax <= 32 ? 32 : 0;
+    }
+#define PP_ZL(C, G, M, K)                                                                                       \
     do {                                                                                                        \
-        auto kfn = zsolve_kernel<C, G, M>;                                                                      \
+        auto kfn = zsolve_kernel<C, G, M, K>;                                                                   \
         if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) \
             return e;                                                                                           \
         kfn<<<grid, block, smem, st>>>(a);                                                                      \
     } while (0)
-#define PP_ZLM(C, G)                   \
-    do {                               \
-        if (mt == 8) PP_ZL(C, G, 8);   \
-        else if (mt == 16) PP_ZL(C, G, 16); \
-        else if (mt == 32 && !C) PP_ZL(C, G, 32); \
-        else PP_ZL(C, G, 0);           \
+#define PP_ZLM(C, G)                                  \
+    do {                                              \
+        if (mt == 8) PP_ZL(C, G, 8, false);           \
+        else if (mt == 16) PP_ZL(C, G, 16, false);    \
+        else if (mt == 32 && !C) PP_ZL(C, G, 32, false); \
+        else if (cap == 8) PP_ZL(C, G, 8, true);      \
+        else if (cap == 12 && C) PP_ZL(C, G, 12, true);  \
+        else if (cap == 16) PP_ZL(C, G, 16, true);    \
+        else if (cap == 24 && !C) PP_ZL(C, G, 24, true); \
+        else if (cap == 32 && !C) PP_ZL(C, G, 32, true); \
+        else PP_ZL(C, G, 0, false);                   \
     } while (0)
     if (cplx && a.data_fp32) PP_ZLM(true, true);
     else if (cplx) PP_ZLM(true, false);
