@@ -204,7 +204,7 @@ PP_D void put(const PPLinePassArgs& a, long off, int plane, Real re, Real im, Re
 }
 
 template <typename Real, int N, int LPC, int FAM, bool INVERSE, bool STRIDED>
-__global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
+__device__ __forceinline__ void lp2_body(const PPLinePassArgs& a)
 {
     using C = typename Vec2<Real>::type;
     constexpr bool FFTK = FAM == F_FFT;
@@ -662,6 +662,27 @@ __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
     }
 }
 
+// the power-of-two lengths, and (with a register bound that leaves room for
+// one more CTA per SM) the lengths with an odd factor, whose final radix-m
+// pass holds up to three butterflies per thread
+constexpr int lpm_min_blocks(int nt) { return 65536 / (84 * nt) > 1 ? 65536 / (84 * nt) : 1; }
+template <typename Real, int N, int LPC, int FAM, bool INVERSE, bool STRIDED>
+__global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
+{
+    lp2_body<Real, N, LPC, FAM, INVERSE, STRIDED>(a);
+}
+template <typename Real, int N, int LPC, int FAM, bool INVERSE, bool STRIDED>
+__global__ void __launch_bounds__(LPC * N / 8, lpm_min_blocks(LPC * N / 8)) lpm_kernel(PPLinePassArgs a)
+{
+    lp2_body<Real, N, LPC, FAM, INVERSE, STRIDED>(a);
+}
+template <typename Real, int N, int LPC, int FAM, bool INVERSE, bool STRIDED>
+constexpr auto pass_kernel()
+{
+    if constexpr ((N & (N - 1)) == 0) return lp2_kernel<Real, N, LPC, FAM, INVERSE, STRIDED>;
+    else return lpm_kernel<Real, N, LPC, FAM, INVERSE, STRIDED>;
+}
+
 template <typename Real, int N, int LPC, int FAM>
 cudaError_t launch_fam(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st)
 {
@@ -669,7 +690,7 @@ cudaError_t launch_fam(const PPLinePassArgs& a, bool inverse, bool strided, cuda
 #define PP_LP2(INV, STR)                                                                                    \
     do {                                                                                                    \
         constexpr size_t smem = smem_bytes<Real, N, LPC, FAM, INV, STR>();                                  \
-        auto kfn = lp2_kernel<Real, N, LPC, FAM, INV, STR>;                                                      \
+        auto kfn = pass_kernel<Real, N, LPC, FAM, INV, STR>();                                              \
         cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
         if (e != cudaSuccess) return e;                                                                     \
         kfn<<<grid, block, smem, st>>>(a);                                                                  \
@@ -687,7 +708,7 @@ cudaError_t launch_half(const PPLinePassArgs& a, cudaStream_t st)
 {
     // the contiguous x pass only: forward real -> half spectra, inverse back
     constexpr size_t smem = smem_bytes<Real, N, LPC, FAM, FAM == F_C2R, false>();
-    auto kfn = lp2_kernel<Real, N, LPC, FAM, FAM == F_C2R, false>;
+    auto kfn = pass_kernel<Real, N, LPC, FAM, FAM == F_C2R, false>();
     cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kfn<<<a.nplanes * a.tiles_per_plane, LPC * N / 8, smem, st>>>(a);
