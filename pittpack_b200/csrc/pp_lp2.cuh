@@ -664,7 +664,8 @@ __device__ __forceinline__ void lp2_body(const PPLinePassArgs& a)
 
 // the power-of-two lengths, and (with a register bound that leaves room for
 // one more CTA per SM) the lengths with an odd factor, whose final radix-m
-// pass holds up to three butterflies per thread
+// pass holds up to three butterflies per thread.  The second argument of
+// __launch_bounds__ is what bounds the registers.
 constexpr int lpm_min_blocks(int nt) { return 65536 / (84 * nt) > 1 ? 65536 / (84 * nt) : 1; }
 template <typename Real, int N, int LPC, int FAM, bool INVERSE, bool STRIDED>
 __global__ void __launch_bounds__(LPC * N / 8) lp2_kernel(PPLinePassArgs a)
@@ -676,10 +677,20 @@ __global__ void __launch_bounds__(LPC * N / 8, lpm_min_blocks(LPC * N / 8)) lpm_
 {
     lp2_body<Real, N, LPC, FAM, INVERSE, STRIDED>(a);
 }
+// the periodic family's 512-point instances (complex lines, half spectra):
+// bounded to 48 registers, five CTAs of 256 threads per SM (measured faster;
+// the real families' instances spill under the same bound and are not)
+template <typename Real, int N, int LPC, int FAM, bool INVERSE, bool STRIDED>
+__global__ void __launch_bounds__(LPC * N / 8, 5) lp2b_kernel(PPLinePassArgs a)
+{
+    lp2_body<Real, N, LPC, FAM, INVERSE, STRIDED>(a);
+}
 template <typename Real, int N, int LPC, int FAM, bool INVERSE, bool STRIDED>
 constexpr auto pass_kernel()
 {
-    if constexpr ((N & (N - 1)) == 0) return lp2_kernel<Real, N, LPC, FAM, INVERSE, STRIDED>;
+    if constexpr (N == 512 && (FAM == F_FFT || FAM == F_R2C || FAM == F_C2R))
+        return lp2b_kernel<Real, N, LPC, FAM, INVERSE, STRIDED>;
+    else if constexpr ((N & (N - 1)) == 0) return lp2_kernel<Real, N, LPC, FAM, INVERSE, STRIDED>;
     else return lpm_kernel<Real, N, LPC, FAM, INVERSE, STRIDED>;
 }
 
