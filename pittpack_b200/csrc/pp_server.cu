@@ -110,14 +110,22 @@ bool handle_busy(const pp_server_s* S, const PooledHandle* ph)
 
 // an idle pooled handle for the shape, or a new one if it fits the budget
 // (evicting idle handles of other shapes, least recently used first);
-// null with *rc == PP_SUCCESS: wait for completions
+// null with *rc == PP_SUCCESS: wait for completions.  A second handle of a
+// shape that already has one (busy) is made only when it fits without
+// evicting: an eviction frees device memory, which waits for the whole
+// device, so waiting for the shape's own handle is the cheaper stall.
 PooledHandle* acquire(pp_server_s* S, const pp_request& r, const ShapeKey& key, int* rc)
 {
     *rc = PP_SUCCESS;
-    for (auto& ph : S->pool)
-        if (ph.key == key && !handle_busy(S, &ph)) return &ph;
+    bool have_shape = false;
+    for (auto& ph : S->pool) {
+        if (ph.key != key) continue;
+        if (!handle_busy(S, &ph)) return &ph;
+        have_shape = true;
+    }
     // a handle holds four 2-complex-per-point buffers plus tables
     const size_t need = (size_t)r.nx * r.ny * r.nz * 8 * sizeof(double) + (1u << 20);
+    if (have_shape && S->pool_bytes + need > S->budget) return nullptr;
     while (S->pool_bytes + need > S->budget) {
         auto victim = S->pool.end();
         for (auto it = S->pool.begin(); it != S->pool.end(); ++it) {
