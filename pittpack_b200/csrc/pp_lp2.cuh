@@ -1,8 +1,11 @@
-// Transform pass for power-of-two line lengths: the same four passes and the
-// same per-family pre/post-processing as pp_linepass.cu (see the reference
+// Transform pass for line lengths N = m 2^k (m = 1, 3, 5, 9, 15; the FFT's
+// power-of-two factor at least 8): the same four passes and the same
+// per-family pre/post-processing as pp_linepass.cu (see the reference
 // citations there), built on the register-resident FFT of pp_fftreg.cuh and
-// specialised at compile time on the boundary family, so that reorders,
-// signs and twiddle selection cost no run-time branches.
+// specialised at compile time on the length and the boundary family, so that
+// reorders, signs and twiddle selection cost no run-time branches.  The
+// power-of-two factor runs as register passes; an odd factor m > 1 as one
+// final Stockham pass of radix m and span 2^k in shared memory.
 //
 //   FFT family (P-P): LPC complex lines per CTA, one FFT of N each.
 //   DCT-II/III, DST-II/III (N-N, D-D): 2 LPC real lines per CTA, packed two
@@ -17,8 +20,9 @@
 // pass a row segment of the tile's lines); (2) each thread gathers its pass-0
 // FFT inputs from the raw tile with the family's reorder folded into the
 // addresses (radix 8 first, so which half a register falls in is known at
-// compile time); (3) FFT; (4) post-processing of pairs (k, N-k), each Z read
-// once, and stores.  The forward x pass's dz^2 scaling is applied to the
+// compile time); (3) FFT, ending with the radix-m pass where m > 1;
+// (4) post-processing of pairs (k, N-k), each Z read once, and stores.  The
+// forward x pass's dz^2 scaling is applied to the
 // outputs (a linear factor), the Dirichlet lift is subtracted (divided by
 // dz^2) from the few raw elements on a Dirichlet face.
 #pragma once
