@@ -417,13 +417,16 @@ def run_serve_leg(args):
             "rates_req_s": SERVE_RATES, "modes": out}
 
 
-def cpu_reference_sample(steps: int, warmup: int, n: int = 128):
-    """The reference's CPU path on one core: one n^3 solve per family it
-    supports per step.  Returns (Mpoints/s, kind, cores, sample text)."""
+REF_FAMILIES = ["PPPPDD", "NNNNDD", "DDDDDD"]
+
+
+def _ref_solver(n: int):
+    """One n^3 solve of the reference's CPU path (its own sources built by
+    oracle/Makefile), or of the oracle restatement when that build is absent.
+    Returns (solve(bc), kind)."""
     import numpy as np
 
     lib = os.path.join(ROOT, "oracle", "_ref", "libppref.so")
-    fams = ["PPPPDD", "NNNNDD", "DDDDDD"]
     rng = np.random.default_rng(11)
     f = rng.uniform(-1, 1, n ** 3)
     out = np.zeros(2 * n ** 3)
@@ -455,24 +458,82 @@ def cpu_reference_sample(steps: int, warmup: int, n: int = 128):
 
         def one(bc):
             O.solve(O.problem(n, n, n, bc), f.reshape(n, n, n))
+    return one, kind
+
+
+def _ref_sample_text(steps: int, n: int, kind: str) -> str:
+    return (f"{steps} step(s) x {len(REF_FAMILIES)} families (PPPPDD, NNNNDD, DDDDDD) of a {n}^3 grid, "
+            f"{'shim FFT in place of FFTW (absent)' if kind == 'reference' else 'oracle restatement'}")
+
+
+def cpu_reference_sample(steps: int, warmup: int, n: int = 128):
+    """The reference's CPU path on one core: one n^3 solve per family it
+    supports per step.  Returns (Mpoints/s, kind, cores, sample text)."""
+    one, kind = _ref_solver(n)
     for _ in range(warmup):
-        one(fams[0])
+        one(REF_FAMILIES[0])
     t0 = time.perf_counter()
-    for s in range(steps):
-        for bc in fams:
+    for _ in range(steps):
+        for bc in REF_FAMILIES:
             one(bc)
     dt = time.perf_counter() - t0
-    pts = steps * len(fams) * n ** 3
-    sample = (f"{steps} step(s) x {len(fams)} families (PPPPDD, NNNNDD, DDDDDD) of a {n}^3 grid, "
-              f"{'shim FFT in place of FFTW (absent)' if kind == 'reference' else 'oracle restatement'}")
-    return pts / dt / 1e6, kind, 1, sample
+    pts = steps * len(REF_FAMILIES) * n ** 3
+    return pts / dt / 1e6, kind, 1, _ref_sample_text(steps, n, kind)
+
+
+def _ref_replica(steps: int, warmup: int, n: int, barrier, queue) -> None:
+    """One single-rank replica of the reference's CPU path, in a process of
+    its own: warm up, wait for the others, time the steps."""
+    try:
+        one, kind = _ref_solver(n)
+        for _ in range(warmup):
+            one(REF_FAMILIES[0])
+        barrier.wait(timeout=600)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            for bc in REF_FAMILIES:
+                one(bc)
+        queue.put((steps * len(REF_FAMILIES) * n ** 3, time.perf_counter() - t0, kind))
+    except Exception as e:  # reported to the parent, which fails the run
+        barrier.abort()
+        queue.put((0, 0.0, f"error: {e}"))
+
+
+def cpu_reference_parallel(steps: int, warmup: int, n: int = 128, workers: int = 0):
+    """The reference's CPU path on all host cores it can use.  The reference
+    runs one MPI rank per core on pencils of one grid; its single-rank build
+    here runs one independent replica per core instead (same arithmetic, no
+    exchanges), all timed together: Mpoints/s = all replicas' points / the
+    slowest replica's time.  Returns (Mpoints/s, kind, cores, sample text)."""
+    import multiprocessing as mp
+
+    if workers <= 0:
+        workers = max(1, min(64, len(os.sched_getaffinity(0))))
+    ctx = mp.get_context("spawn")
+    barrier, queue = ctx.Barrier(workers), ctx.Queue()
+    procs = [ctx.Process(target=_ref_replica, args=(steps, warmup, n, barrier, queue)) for _ in range(workers)]
+    for p in procs:
+        p.start()
+    try:
+        res = [queue.get(timeout=1800) for _ in range(workers)]
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+    bad = [k for _, _, k in res if k.startswith("error")]
+    if bad:
+        raise RuntimeError(f"reference replica failed: {bad[0]}")
+    pts = sum(r[0] for r in res)
+    dt = max(r[1] for r in res)
+    kind = res[0][2]
+    sample = f"{workers} concurrent single-rank replicas (one per core), each " + _ref_sample_text(steps, n, kind)
+    return pts / dt / 1e6, kind, workers, sample
 
 
 def run_reference(args):
     rank, _, world = env_rank()
     if rank != 0:
         return 0
-    v, kind, cores, sample = cpu_reference_sample(max(1, args.steps), max(0, min(args.warmup, 1)))
+    v, kind, cores, sample = cpu_reference_parallel(max(1, args.steps), max(0, min(args.warmup, 1)))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
