@@ -171,10 +171,11 @@ int pp_set_tuning(pp_handle h, const pp_tuning* t);
 int pp_get_tuning(pp_handle h, pp_tuning* t);
 /* autotuner, no counterpart in the reference: times 'reps' solves of the
  * assigned RHS for each candidate lane count of the z solve, then each
- * number of z systems per CTA and, when x or y is not a power of two, each
- * line tile of the generic transform kernel (one coordinate after the other), keeps the fastest shape in the handle and
- * reports it with its milliseconds per solve.  Synchronises the stream; the
- * handle's solution is overwritten. */
+ * number of z systems per CTA and, when x or y runs the generic transform
+ * kernel (lengths other than m 2^k, m = 1, 3, 5, 9, 15), each of its line
+ * tiles (one coordinate after the other); keeps the fastest shape in the
+ * handle and reports it with its milliseconds per solve.  Synchronises the
+ * stream; the handle's solution is overwritten. */
 int pp_autotune(pp_handle h, int reps, pp_tuning* chosen, double* best_ms);
 
 /* ---- batched solves (no counterpart in the reference, which solves one grid
