@@ -60,7 +60,8 @@ typedef struct pp_solver_s* pp_handle;
  * src/pencilDcmp.cpp:5066-5105). */
 typedef struct {
     int zsolve_lanes; /* lanes sharing one z system: 1..32, a power of two */
-    int line_tile;    /* lines per CTA of the generic (non-power-of-two) transform kernel, 1..32 */
+    int line_tile;    /* lines per CTA of the generic transform kernel (lengths other than
+                         m 2^k, m = 1, 3, 5, 9, 15), 1..32 */
     int zsolve_tile;  /* z systems (adjacent kx) per CTA of the z solve: 1..32, a power of two */
 } pp_tuning;
 
