@@ -122,8 +122,6 @@ void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* thre
 int pp_zsolve_valid_lanes(int nz, int P);
 size_t pp_zsolve_smem_p(int TS, int nz, bool cplx, int P);
 
-size_t pp_zsolve_smem(int TS, int nz, bool cplx);
-
 // FP64 residual r = f dz^2 - lift - A u of the refined solve (pp_mixed.cu)
 struct PPResidArgs {
     const double* f;   // real RHS, unscaled

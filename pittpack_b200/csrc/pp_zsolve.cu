@@ -640,11 +640,6 @@ void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads)
     *threads = ts * P < 32 ? 32 : ts * P;
 }
 
-size_t pp_zsolve_smem(int TS, int nz, bool cplx)
-{
-    return pp_zsolve_smem_p(TS, nz, cplx, pp_zsolve_lanes(nz, cplx, false));
-}
-
 // a lane count the kernel accepts: a power of two <= 32 leaving every lane at
 // least two rows
 int pp_zsolve_valid_lanes(int nz, int P)
