@@ -57,12 +57,13 @@ N_GRID = 512
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
-# algorithmic bytes per point of each solve kernel for a real RHS:
-# (read + write), see DESIGN.md "Kernels and their rooflines"
+# the solve's stages in the order pp_timing_end reports them; their
+# algorithmic bytes per point (read + write) are kernel_bytes_per_point()
 KERNEL_NAMES = ["x_forward", "y_forward", "z_solve", "y_inverse", "x_inverse", "residual"]
-# DRAM bytes moved / algorithmic bytes per stage, from one ncu capture of the
-# FP64 solve (512 x 512 x 128, NN family; profiles/solve_kernels_dram_traffic_512x512x128.md):
-# reads equal the algorithmic bytes, writes read low by what is still in L2
+# DRAM bytes moved / algorithmic bytes per stage, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of the FP64 solve at
+# 512 x 512 x 128, NN family: reads equal the algorithmic bytes, writes read
+# low by what is still in L2 when a kernel ends
 DRAM_OVER_ALGORITHMIC = {"x_forward": 14.62 / 16, "y_forward": 14.69 / 16, "z_solve": 14.11 / 16,
                          "y_inverse": 14.63 / 16, "x_inverse": 22.15 / 24}
 
