@@ -21,11 +21,13 @@
 //   * a group of P lanes (P = 32 / systems per warp) solves one system by the
 //     partition method: lane L owns a contiguous block of M ~ nz/P rows and
 //     eliminates it so that every interior unknown is expressed through the
-//     block's first and last unknown (forward sweep with one division per
-//     row, then a backward sweep), leaving two equations per lane.  Interior
-//     rows have the same coefficients in every block, so the pivots and
-//     spikes of a block depend only on lambda; the CTA builds them into a
-//     shared table (one reciprocal per entry) that every lane reads;
+//     block's first and last unknown (a forward sweep, a backward sweep for
+//     the first row, a recovery sweep), leaving two equations per lane; the
+//     rows stay in registers where the counts allow.  Interior rows have the
+//     same coefficients in every block, so the pivots and spikes of a block
+//     depend only on lambda; the CTA builds them into a shared table (one
+//     reciprocal per entry) that every lane reads, and the sweeps divide only
+//     on the system's last row;
 //   * eliminating each lane's first unknown leaves a P-row tridiagonal system
 //     in the lanes' last unknowns, solved by parallel cyclic reduction over
 //     warp shuffles (periodic systems through Sherman-Morrison); each lane
