@@ -94,6 +94,19 @@ int pp_set_box(pp_handle h, const double X[6]);
  * zmax, letters 'P' 'N' 'D'.  x and y take P-P, N-N, D-D, N-D or D-N; z takes
  * D/N at either end or P-P. */
 int pp_assign_boundary(pp_handle h, const char bc[6]);
+/* Non-homogeneous boundary data, no counterpart in the reference (whose
+ * modifyRhsDirichlet, src/pencilDcmp.cpp:4623-4835, adds only its own
+ * manufactured solution): values g on face 'face' (0..5 = xmin, xmax, ymin,
+ * ymax, zmin, zmax, the order of the bc string) -- the boundary value on a
+ * Dirichlet face, the outward normal derivative on a Neumann face -- at the
+ * face's cell centres: x faces g[j + ny k], y faces g[i + nx k], z faces
+ * g[i + nx j].  They enter the right-hand side through the ghost-cell
+ * relations (Dirichlet u_ghost = 2 g - u_0, Neumann u_ghost = u_0 + h g)
+ * with the face's stencil weight ((dz/dx)^2, (dz/dy)^2, 1).  A face with data
+ * replaces the manufactured lift of the dirichlet_lift option on that face;
+ * g = NULL clears it.  The data are copied.  After pp_assign_boundary
+ * (PP_NOT_READY before); a periodic face takes none (PP_INPUT_ARGS). */
+int pp_set_face_values(pp_handle h, int face, const double* g);
 
 int pp_default_options(pp_options* opt);
 int pp_set_options(pp_handle h, const pp_options* opt);

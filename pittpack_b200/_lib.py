@@ -64,6 +64,7 @@ def load():
         "pp_destroy": ([H], i),
         "pp_set_box": ([H, dp], i),
         "pp_assign_boundary": ([H, ctypes.c_char_p], i),
+        "pp_set_face_values": ([H, i, ctypes.c_void_p], i),
         "pp_default_options": ([ctypes.POINTER(Options)], i),
         "pp_set_options": ([H, ctypes.POINTER(Options)], i),
         "pp_get_options": ([H, ctypes.POINTER(Options)], i),

@@ -97,6 +97,9 @@ struct pp_solver_s {
     int last_sweeps = 0;
     DevBuf lift[6];
     PPLift liftv{};
+    // caller's boundary data per face (xmin, xmax, ymin, ymax, zmin, zmax);
+    // empty: none (pp_set_face_values)
+    std::vector<double> uface[6];
     std::mutex mu;
     std::string last_error;
     // live per-stage timing (pp_timing_begin / pp_timing_end): events from a
@@ -219,13 +222,17 @@ double exact_value(double omega, double x, int tg)
     return 0.0;
 }
 
-// face corrections of modifyRhsDirichlet (src/pencilDcmp.cpp:4623-4835),
-// evaluated with the reference's expressions
+// face corrections subtracted from the dz^2-scaled RHS: the caller's boundary
+// data where pp_set_face_values set some, else (option dirichlet_lift) the
+// manufactured-solution faces of modifyRhsDirichlet
+// (src/pencilDcmp.cpp:4623-4835), evaluated with the reference's expressions
 int build_lift(pp_solver_s* h)
 {
     for (auto& b : h->lift) b.free();
     h->liftv = PPLift{};
-    if (!h->opt.dirichlet_lift) return PP_SUCCESS;
+    bool user = false;
+    for (int f = 0; f < 6; ++f) user |= !h->uface[f].empty() && h->bc[f] != 'P';
+    if (!h->opt.dirichlet_lift && !user) return PP_SUCCESS;
     const int nx = h->nx, ny = h->ny, nz = h->nz;
     const double pi = 4. * atan(1.0);
     const double Xa = h->box[0], Ya = h->box[2], Za = h->box[4];
@@ -247,9 +254,10 @@ int build_lift(pp_solver_s* h)
         return PP_SUCCESS;
     };
     int rc;
-    if (h->bc[4] == 'D' || h->bc[5] == 'D') {
+    const bool manufactured = h->opt.dirichlet_lift != 0;
+    if (manufactured && (h->bc[4] == 'D' || h->bc[5] == 'D')) {
         for (int face = 0; face < 2; ++face) {
-            if (h->bc[4 + face] != 'D') continue;
+            if (h->bc[4 + face] != 'D' || !h->uface[4 + face].empty()) continue;
             std::vector<double> v((size_t)nx * ny);
             const double z = face == 0 ? Za : Za + (nz - 1) * c3 + c3;
             for (int i = 0; i < nx; ++i) {
@@ -263,8 +271,8 @@ int build_lift(pp_solver_s* h)
             if ((rc = upload(face, v)) != PP_SUCCESS) return rc;
         }
     }
-    for (int face = 0; face < 2; ++face) {
-        if (h->bc[face] != 'D') continue;
+    for (int face = 0; face < 2 && manufactured; ++face) {
+        if (h->bc[face] != 'D' || !h->uface[face].empty()) continue;
         std::vector<double> v((size_t)ny * nz);
         const double x = face == 0 ? Xa : Xa + ((nx - 1) + 1) * c1;
         for (int k = 0; k < nz; ++k) {
@@ -277,8 +285,8 @@ int build_lift(pp_solver_s* h)
         }
         if ((rc = upload(2 + face, v)) != PP_SUCCESS) return rc;
     }
-    for (int face = 0; face < 2; ++face) {
-        if (h->bc[2 + face] != 'D') continue;
+    for (int face = 0; face < 2 && manufactured; ++face) {
+        if (h->bc[2 + face] != 'D' || !h->uface[2 + face].empty()) continue;
         std::vector<double> v((size_t)nx * nz);
         const double y = face == 0 ? Ya : Ya + ((ny - 1) + 1) * c2;
         for (int k = 0; k < nz; ++k) {
@@ -290,6 +298,24 @@ int build_lift(pp_solver_s* h)
             }
         }
         if ((rc = upload(4 + face, v)) != PP_SUCCESS) return rc;
+    }
+    // the caller's data through the ghost-cell relations of the 7-point operator
+    // scaled by dz^2: a face's neighbour term has weight w = (dz/dx)^2,
+    // (dz/dy)^2 or 1; Dirichlet u_ghost = 2 g - u_0 moves 2 w g to the right-hand
+    // side, Neumann (outward derivative g) u_ghost = u_0 + h g moves w h g
+    {
+        const double wgt[3] = {(c3 / c1) * (c3 / c1), (c3 / c2) * (c3 / c2), 1.0};
+        const double hh[3] = {c1, c2, c3};
+        for (int f = 0; f < 6; ++f) {
+            if (h->uface[f].empty() || h->bc[f] == 'P') continue;
+            const int d = f / 2;
+            const double c = h->bc[f] == 'D' ? 2.0 * wgt[d] : wgt[d] * hh[d];
+            std::vector<double> v(h->uface[f].size());
+            for (size_t q = 0; q < v.size(); ++q) v[q] = c * h->uface[f][q];
+            // device slots: z faces 0, 1; x faces 2, 3; y faces 4, 5
+            const int slot = d == 2 ? f - 4 : (d == 0 ? 2 + f : 4 + (f - 2));
+            if ((rc = upload(slot, v)) != PP_SUCCESS) return rc;
+        }
     }
     PPLift& L = h->liftv;
     L.z0 = h->lift[0].as<double>();
@@ -946,6 +972,26 @@ int pp_assign_boundary(pp_handle h, const char bc[6])
     int rc = rebuild_tables(h);
     h->have_bc = rc == PP_SUCCESS;
     return rc;
+}
+
+int pp_set_face_values(pp_handle h, int face, const double* g)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (face < 0 || face > 5) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (!h->have_bc) return PP_NOT_READY;
+    if (h->bc[face] == 'P') return PP_INPUT_ARGS;
+    const int d = face / 2;
+    const size_t n = d == 0 ? (size_t)h->ny * h->nz : (d == 1 ? (size_t)h->nx * h->nz : (size_t)h->nx * h->ny);
+    if (g) {
+        for (size_t q = 0; q < n; ++q)
+            if (!std::isfinite(g[q])) return PP_INPUT_ARGS;
+        h->uface[face].assign(g, g + n);
+    } else {
+        h->uface[face].clear();
+    }
+    cudaSetDevice(h->device);
+    return build_lift(h);
 }
 
 int pp_set_options(pp_handle h, const pp_options* opt)

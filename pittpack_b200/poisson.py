@@ -46,6 +46,22 @@ class PoissonGPU:
         check(self._L.pp_assign_boundary(self._h, b), "assignBoundary")
         self.bc = b.decode()
 
+    def setFaceValues(self, face: int, g) -> None:
+        """Boundary data of one face (0..5 = xmin, xmax, ymin, ymax, zmin,
+        zmax): the value on a Dirichlet face, the outward normal derivative on
+        a Neumann face, at the face's cell centres -- shape (nz, ny) for x
+        faces, (nz, nx) for y faces, (ny, nx) for z faces; None clears it."""
+        if g is None:
+            check(self._L.pp_set_face_values(self._h, int(face), None), "setFaceValues")
+            return
+        if not 0 <= int(face) < 6:
+            raise PittPackError(_lib.PP_INPUT_ARGS, f"setFaceValues: face {face} is not 0..5")
+        shape = [(self.nz, self.ny), (self.nz, self.nx), (self.ny, self.nx)][int(face) // 2]
+        a = np.ascontiguousarray(g, dtype=np.float64)
+        if a.size != shape[0] * shape[1]:
+            raise PittPackError(_lib.PP_INPUT_ARGS, f"setFaceValues: face {face} needs {shape} values")
+        check(self._L.pp_set_face_values(self._h, int(face), a.ctypes.data), "setFaceValues")
+
     def setBox(self, X) -> None:
         x = np.ascontiguousarray(X, dtype=np.float64)
         if x.size != 6:
