@@ -76,6 +76,8 @@ typedef struct {
     int compat_zero_mode; /* 1 (default): reference zero-mode row replacement, src/triDiag.cpp:1753-1776 */
     int dirichlet_lift;   /* 1 (default): reference modifyRhsDirichlet, src/pencilDcmp.cpp:4623-4835 */
     int z_solver;         /* PP_ZSOLVE_DIRECT (default) or PP_ZSOLVE_MULTIGRID (plain FP64 solve only) */
+    int zero_mean;        /* 0 (default) or 1: subtract the mean of the solution's real part, the
+                             reference's ZERO_MEAN (subtractMeanValue, src/pencilDcmp.cpp:5649-5683) */
 } pp_options;
 
 /* the reference's PittPackGetErrorEnum (src/pencilDcmp.cpp:4869-4913) */

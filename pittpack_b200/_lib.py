@@ -30,6 +30,7 @@ class Options(ctypes.Structure):
         ("compat_zero_mode", ctypes.c_int),
         ("dirichlet_lift", ctypes.c_int),
         ("z_solver", ctypes.c_int),
+        ("zero_mean", ctypes.c_int),
     ]
 
 

@@ -136,6 +136,11 @@ struct PPResidArgs {
     double* usum;      // FP64 sum of u over the grid, or null
 };
 cudaError_t pp_launch_resid(const PPResidArgs& a, cudaStream_t st);
+// zero-mean solution (pp_mean.cu): the mean of the real parts of the n
+// complex-interleaved values of P is subtracted from them; scratch holds
+// pp_zero_mean_scratch_doubles() doubles
+size_t pp_zero_mean_scratch_doubles();
+cudaError_t pp_launch_zero_mean(double* P, long n, double* scratch, cudaStream_t st);
 // Singular problems: keep the null-space constant of the refined solution at
 // the value implied by the pinned FP64 zero-mode solve of b (see pp_mixed.cu).
 cudaError_t pp_launch_zero_mode_anchor(double* zcol, int nz, const double* usum, double* mstar, double zscale,

@@ -94,6 +94,7 @@ struct pp_solver_s {
     DevBuf psum;   // refined solve: per-plane sums / zero-mode column (nz doubles)
     DevBuf zero1;  // one double 0.0 (eigen table of the zero-mode system)
     DevBuf mgstats;  // multigrid z solve: max cycles, unconverged systems (2 ints)
+    DevBuf zmean;    // zero-mean option: partial sums and the mean
     int last_sweeps = 0;
     DevBuf lift[6];
     PPLift liftv{};
@@ -529,6 +530,16 @@ int tuned_lines(const pp_solver_s* h, int nfft)
     return pick_lines(nfft);
 }
 
+// the zero-mean option (the reference's ZERO_MEAN): after the solve, the mean
+// of the solution's real part is subtracted from it
+int zero_mean(pp_solver_s* h)
+{
+    if (!h->opt.zero_mean) return PP_SUCCESS;
+    double* P = h->ext_out ? h->ext_out : h->out.as<double>();
+    const cudaError_t e = pp_launch_zero_mean(P, (long)h->nx * h->ny * h->nz, h->zmean.as<double>(), h->stream);
+    return e == cudaSuccess ? PP_SUCCESS : set_cuda_error(h, e, PP_CUDA_ERROR);
+}
+
 int launch_solve(pp_solver_s* h)
 {
     const int nx = h->nx, ny = h->ny, nz = h->nz;
@@ -661,7 +672,7 @@ int launch_solve(pp_solver_s* h)
     if ((e = line_pass(a4, h->tx, true, false, s_cplx, true, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_INV_X);
     stage_done(h, SLOT_XI, t0);
-    return PP_SUCCESS;
+    return zero_mean(h);
 }
 
 bool has_zero_mode(int kx, int ky)
@@ -839,7 +850,7 @@ int launch_mixed(pp_solver_s* h)
         stage_done(h, SLOT_XI, t0);
     }
     h->last_sweeps = sweeps;
-    return PP_SUCCESS;
+    return zero_mean(h);
 }
 
 }  // namespace
@@ -890,6 +901,7 @@ int pp_default_options(pp_options* opt)
     opt->compat_zero_mode = 1;
     opt->dirichlet_lift = 1;
     opt->z_solver = PP_ZSOLVE_DIRECT;
+    opt->zero_mean = 0;
     return PP_SUCCESS;
 }
 
@@ -939,6 +951,7 @@ int pp_destroy(pp_handle h)
     h->psum.free();
     h->zero1.free();
     h->mgstats.free();
+    h->zmean.free();
     h->tx.twf.free(); h->tx.csf.free(); h->ty.twf.free(); h->ty.csf.free();
     h->tx.tw.free(); h->tx.cs.free(); h->tx.eig.free();
     h->ty.tw.free(); h->ty.cs.free(); h->ty.eig.free();
@@ -1001,8 +1014,17 @@ int pp_set_options(pp_handle h, const pp_options* opt)
     if (opt->precision != PP_PRECISION_FP64 && opt->precision != PP_PRECISION_MIXED) return PP_INPUT_ARGS;
     if (opt->max_sweeps < 0 || opt->max_sweeps > 16) return PP_INPUT_ARGS;
     if (opt->z_solver != PP_ZSOLVE_DIRECT && opt->z_solver != PP_ZSOLVE_MULTIGRID) return PP_INPUT_ARGS;
+    if (opt->zero_mean != 0 && opt->zero_mean != 1) return PP_INPUT_ARGS;
     std::lock_guard<std::mutex> g(h->mu);
     const bool lift_changed = opt->dirichlet_lift != h->opt.dirichlet_lift;
+    if (opt->zero_mean && !h->zmean.p) {
+        // allocated here, never inside a solve (which may be captured in a graph)
+        cudaSetDevice(h->device);
+        if (h->zmean.alloc(pp_zero_mean_scratch_doubles() * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            return PP_ALLOCATION_FAIL;
+        }
+    }
     h->opt = *opt;
     if (lift_changed && h->have_bc) {
         cudaSetDevice(h->device);

@@ -54,7 +54,7 @@ def test_status_strings_and_null_arguments(lib):
     assert L.pp_create(8, 8, 2, ctypes.byref(h)) == _lib.PP_INPUT_ARGS
     o = _lib.Options()
     assert L.pp_default_options(ctypes.byref(o)) == 0
-    assert o.compat_zero_mode == 1 and o.dirichlet_lift == 1 and o.precision == 0
+    assert o.compat_zero_mode == 1 and o.dirichlet_lift == 1 and o.precision == 0 and o.zero_mean == 0
 
 
 def test_no_gpu_here_reports_init_failure(lib):
