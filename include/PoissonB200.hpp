@@ -53,6 +53,15 @@ class PoissonB200 {
     void setBox(const double X[6]) { check(pp_set_box(h_, X), "setBox"); }
     void setCoords(int /*dir*/) {}  // one rank owns the whole box
     void setOptions(const pp_options& o) { check(pp_set_options(h_, &o), "setOptions"); }
+    pp_options options() const
+    {
+        pp_options o;
+        check(pp_get_options(h_, &o), "options");
+        return o;
+    }
+    // boundary data of one face (0..5 = xmin .. zmax), see pp_set_face_values;
+    // nullptr clears it
+    void setFaceValues(int face, const double* g) { check(pp_set_face_values(h_, face, g), "setFaceValues"); }
     void assignRhs(const double* rhs) { check(pp_assign_rhs(h_, rhs), "assignRhs"); }
     void assignRhsComplex(const double* rhs) { check(pp_assign_rhs_complex(h_, rhs), "assignRhsComplex"); }
     void pittPack() { check(pp_solve(h_), "pittPack"); }

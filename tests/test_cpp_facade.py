@@ -28,6 +28,11 @@ int main() {
         double X[6] = {0, 1.0, 0, 1.0, 0, 1.0};
         M->setBox(X);
         M->setCoords(2);
+        pp_options o = M->options();
+        o.zero_mean = 1;
+        M->setOptions(o);
+        std::vector<double> g(Nx * Ny, 0.25);
+        M->setFaceValues(4, g.data());
         M->assignRhs(rhs.data());
         M->pittPack();
         std::vector<double> P(2 * Nx * Ny * Nz);
