@@ -34,6 +34,8 @@ class Problem(ctypes.Structure):
         ("box", ctypes.c_double * 6),
         ("compat_zero_mode", ctypes.c_int),
         ("dirichlet_lift", ctypes.c_int),
+        ("face", ctypes.c_void_p * 6),
+        ("zero_mean", ctypes.c_int),
     ]
 
 
@@ -74,7 +76,11 @@ def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-def problem(nx, ny, nz, bc, box=(0, 1, 0, 1, 0, 1), compat_zero_mode=1, dirichlet_lift=1) -> Problem:
+def problem(nx, ny, nz, bc, box=(0, 1, 0, 1, 0, 1), compat_zero_mode=1, dirichlet_lift=1, faces=None,
+            zero_mean=0) -> Problem:
+    """faces: {face 0..5: array} of boundary data (Dirichlet values / Neumann
+    outward derivatives, shaped (nz, ny), (nz, nx) or (ny, nx) for x, y, z
+    faces); zero_mean: subtract the solution's mean (ZERO_MEAN)."""
     p = Problem()
     p.nx, p.ny, p.nz = nx, ny, nz
     p.bc = bc.encode() if isinstance(bc, str) else bytes(bc)
@@ -82,6 +88,13 @@ def problem(nx, ny, nz, bc, box=(0, 1, 0, 1, 0, 1), compat_zero_mode=1, dirichle
         p.box[i] = float(box[i])
     p.compat_zero_mode = int(compat_zero_mode)
     p.dirichlet_lift = int(dirichlet_lift)
+    p.zero_mean = int(zero_mean)
+    keep = []
+    for f, g in (faces or {}).items():
+        a = np.ascontiguousarray(g, dtype=np.float64).ravel()
+        keep.append(a)
+        p.face[int(f)] = a.ctypes.data
+    p._keep = keep  # the face arrays live as long as the problem
     return p
 
 

@@ -595,7 +595,7 @@ static void modify_rhs_dirichlet(const ppo_problem* pb, double* P)
     int t2 = ref_tag_z(pb->bc);
     double x, y, z;
 #define PRE(i, j, k) P[2 * ((long)(i) + (long)nx * (j) + (long)nx * ny * (k))]
-    if (pb->bc[4] == 'D') {
+    if (pb->bc[4] == 'D' && !pb->face[4]) {
         z = Za;
         int k = 0;
         for (int i = 0; i < nx; ++i) {
@@ -608,7 +608,7 @@ static void modify_rhs_dirichlet(const ppo_problem* pb, double* P)
             }
         }
     }
-    if (pb->bc[5] == 'D') {
+    if (pb->bc[5] == 'D' && !pb->face[5]) {
         z = Za + (nz - 1) * c3 + c3;
         int k = nz - 1;
         for (int i = 0; i < nx; ++i) {
@@ -621,7 +621,7 @@ static void modify_rhs_dirichlet(const ppo_problem* pb, double* P)
             }
         }
     }
-    if (pb->bc[0] == 'D') {
+    if (pb->bc[0] == 'D' && !pb->face[0]) {
         x = Xa;
         int i = 0;
         for (int k = 0; k < nz; ++k) {
@@ -634,7 +634,7 @@ static void modify_rhs_dirichlet(const ppo_problem* pb, double* P)
             }
         }
     }
-    if (pb->bc[1] == 'D') {
+    if (pb->bc[1] == 'D' && !pb->face[1]) {
         int i = nx - 1;
         x = Xa + (i + 1) * c1;
         for (int k = 0; k < nz; ++k) {
@@ -647,7 +647,7 @@ static void modify_rhs_dirichlet(const ppo_problem* pb, double* P)
             }
         }
     }
-    if (pb->bc[2] == 'D') {
+    if (pb->bc[2] == 'D' && !pb->face[2]) {
         y = Ya;
         int j = 0;
         for (int k = 0; k < nz; ++k) {
@@ -660,7 +660,7 @@ static void modify_rhs_dirichlet(const ppo_problem* pb, double* P)
             }
         }
     }
-    if (pb->bc[3] == 'D') {
+    if (pb->bc[3] == 'D' && !pb->face[3]) {
         int j = ny - 1;
         y = Ya + (j + 1) * c2;
         for (int k = 0; k < nz; ++k) {
@@ -671,6 +671,38 @@ static void modify_rhs_dirichlet(const ppo_problem* pb, double* P)
                                - 2. * exact_value(omega[0], x, t0) * exact_value(omega[1], y, t1)
                                      * exact_value(omega[2], z, t2);
             }
+        }
+    }
+#undef PRE
+}
+
+/* the caller's boundary data (ppo_problem.face): the right-hand-side share of
+ * each face's ghost cells, subtracted from the dz^2-scaled RHS on the first
+ * cell layer */
+static void user_faces(const ppo_problem* pb, double* P)
+{
+    int nx = pb->nx, ny = pb->ny, nz = pb->nz;
+    double h[3] = {-(pb->box[0] - pb->box[1]) / nx, -(pb->box[2] - pb->box[3]) / ny,
+                   -(pb->box[4] - pb->box[5]) / nz};
+    double w[3] = {(h[2] / h[0]) * (h[2] / h[0]), (h[2] / h[1]) * (h[2] / h[1]), 1.0};
+#define PRE(i, j, k) P[2 * ((long)(i) + (long)nx * (j) + (long)nx * ny * (k))]
+    for (int f = 0; f < 6; ++f) {
+        const double* g = pb->face[f];
+        if (!g || pb->bc[f] == 'P') continue;
+        int d = f / 2;
+        double c = pb->bc[f] == 'D' ? 2.0 * w[d] : w[d] * h[d];
+        if (d == 0) {
+            int i = (f & 1) ? nx - 1 : 0;
+            for (int k = 0; k < nz; ++k)
+                for (int j = 0; j < ny; ++j) PRE(i, j, k) -= c * g[j + (long)ny * k];
+        } else if (d == 1) {
+            int j = (f & 1) ? ny - 1 : 0;
+            for (int k = 0; k < nz; ++k)
+                for (int i = 0; i < nx; ++i) PRE(i, j, k) -= c * g[i + (long)nx * k];
+        } else {
+            int k = (f & 1) ? nz - 1 : 0;
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) PRE(i, j, k) -= c * g[i + (long)nx * j];
         }
     }
 #undef PRE
@@ -703,6 +735,7 @@ int ppo_solve(const ppo_problem* pb, const double* rhs_re, const double* rhs_im,
         P[2 * p + 1] = rhs_im ? rhs_im[p] * c3 * c3 : 0.0;
     }
     if (pb->dirichlet_lift) modify_rhs_dirichlet(pb, P);
+    user_faces(pb, P);
 
     int nmax = nx > ny ? nx : ny;
     if (nz > nmax) nmax = nz;
@@ -781,6 +814,13 @@ int ppo_solve(const ppo_problem* pb, const double* rhs_re, const double* rhs_im,
     dft_plan_free(&hx);
     dft_plan_free(&hy);
     free(re); free(im); free(t);
+    if (pb->zero_mean) {
+        /* subtractMeanValue (src/pencilDcmp.cpp:5649-5683) */
+        long double sum = 0.0L;
+        for (long p = 0; p < n; ++p) sum += P[2 * p];
+        double mean = (double)(sum / n);
+        for (long p = 0; p < n; ++p) P[2 * p] -= mean;
+    }
     return 0;
 }
 

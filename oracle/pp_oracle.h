@@ -26,6 +26,14 @@ typedef struct {
     double box[6];       /* Xa Xb Ya Yb Za Zb */
     int compat_zero_mode; /* 1: the reference's zero-mode row replacement */
     int dirichlet_lift;   /* 1: the reference's modifyRhsDirichlet */
+    /* caller's boundary data per face (order of bc; NULL: none): Dirichlet
+     * values or Neumann outward derivatives at the face's cell centres, x
+     * faces [j + ny k], y faces [i + nx k], z faces [i + nx j]; a face with
+     * data takes no manufactured lift.  Not in the reference: the ghost-cell
+     * relations u_g = 2 g - u_0 (D) and u_g = u_0 + h g (N) with the face's
+     * stencil weight (dz/dx)^2, (dz/dy)^2 or 1. */
+    const double* face[6];
+    int zero_mean;        /* 1: the reference's ZERO_MEAN (subtractMeanValue) */
 } ppo_problem;
 
 int ppo_kind_from_bc(char lo, char hi);

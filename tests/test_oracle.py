@@ -82,3 +82,26 @@ def test_manufactured_solution_converges_second_order(bc):
         errs.append(e)
     rates = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
     assert min(rates) > 1.8, (errs, rates)
+
+
+@pytest.mark.parametrize("case", [(8, 6, 5, "DDDDDD"), (8, 6, 5, "NNDDDN"), (6, 5, 7, "DNNDND"), (8, 8, 4, "NDDNDD")])
+def test_oracle_face_values_give_the_exact_discrete_solution(case):
+    # the construction of the GPU test: f and the face data from a smooth u
+    # through the ghost-cell relations, so that u solves the discrete problem
+    from test_gpu_face_values import _problem
+
+    nx, ny, nz, bc = case
+    box = (0.0, 1.0, -0.5, 1.0, 0.2, 1.0)
+    u, f, faces = _problem(nx, ny, nz, bc, box)
+    P = O.solve(O.problem(nx, ny, nz, bc, box=box, compat_zero_mode=0, faces=faces), f)
+    assert np.linalg.norm(P.real - u) / np.linalg.norm(u) <= 1e-12
+
+
+def test_oracle_zero_mean_subtracts_the_solution_mean():
+    nx, ny, nz, bc = 8, 6, 5, "NNNNNN"
+    f = np.random.default_rng(2).uniform(-1, 1, (nz, ny, nx))
+    f -= f.mean()
+    P0 = O.solve(O.problem(nx, ny, nz, bc, compat_zero_mode=0), f)
+    P1 = O.solve(O.problem(nx, ny, nz, bc, compat_zero_mode=0, zero_mean=1), f)
+    assert np.allclose(P1.real, P0.real - P0.real.mean(), rtol=0, atol=1e-14 * np.abs(P0.real).max())
+    assert abs(P1.real.mean()) <= 1e-14 * np.abs(P0.real).max()
