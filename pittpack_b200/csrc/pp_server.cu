@@ -301,11 +301,17 @@ extern "C" int pp_server_wait(pp_server S, unsigned long long ticket, double* la
 {
     if (!S) return PP_INVALID_HANDLE;
     std::unique_lock<std::mutex> lk(S->mu);
-    auto it = S->results.find(ticket);
+    if (S->results.find(ticket) == S->results.end()) return PP_INPUT_ARGS;
+    // a ticket is collected once: a second waiter on it (another thread) sees
+    // its entry vanish and returns PP_INPUT_ARGS instead of waiting for good
+    auto it = S->results.end();
+    S->cv.wait(lk, [&] {
+        it = S->results.find(ticket);
+        return it == S->results.end() || it->second.done;
+    });
     if (it == S->results.end()) return PP_INPUT_ARGS;
-    S->cv.wait(lk, [&] { return S->results[ticket].done; });
-    const Result res = S->results[ticket];
-    S->results.erase(ticket);
+    const Result res = it->second;
+    S->results.erase(it);
     if (latency_ms) *latency_ms = res.latency_ms;
     if (precision) *precision = res.precision;
     return res.status;
