@@ -175,13 +175,17 @@ class PoissonGPU:
     def assignRhsAsync(self, rhs: np.ndarray) -> None:
         """Real RHS copied on the handle's stream without waiting; keep rhs
         alive and unchanged until the stream has passed the next solve."""
-        assert rhs.dtype == np.float64 and rhs.flags.c_contiguous and rhs.size == self.nx * self.ny * self.nz
+        if not (isinstance(rhs, np.ndarray) and rhs.dtype == np.float64 and rhs.flags.c_contiguous
+                and rhs.size == self.nx * self.ny * self.nz):
+            raise PittPackError(_lib.PP_INPUT_ARGS, "assignRhsAsync needs a contiguous float64 array of nx*ny*nz")
         check(self._L.pp_assign_rhs_async(self._h, rhs.ctypes.data), "pp_assign_rhs_async")
 
     def getSolutionAsync(self, out: np.ndarray) -> None:
         """Solution copied into out (complex128, nx*ny*nz) on the handle's
         stream without waiting; synchronize() before reading it."""
-        assert out.dtype == np.complex128 and out.flags.c_contiguous and out.size == self.nx * self.ny * self.nz
+        if not (isinstance(out, np.ndarray) and out.dtype == np.complex128 and out.flags.c_contiguous
+                and out.size == self.nx * self.ny * self.nz):
+            raise PittPackError(_lib.PP_INPUT_ARGS, "getSolutionAsync needs a contiguous complex128 array of nx*ny*nz")
         check(self._L.pp_get_solution_async(self._h, out.ctypes.data), "pp_get_solution_async")
 
     def setTuning(self, zsolve_lanes: int = 0, line_tile: int = 0, zsolve_tile: int = 0) -> None:
