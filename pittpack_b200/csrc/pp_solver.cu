@@ -1055,6 +1055,7 @@ int pp_get_options(pp_handle h, pp_options* opt)
 {
     if (!h) return PP_INVALID_HANDLE;
     if (!opt) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
     *opt = h->opt;
     return PP_SUCCESS;
 }
@@ -1312,9 +1313,12 @@ int pp_workspace_bytes(pp_handle h, size_t* bytes)
 {
     if (!h) return PP_INVALID_HANDLE;
     if (!bytes) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
     size_t b = h->rhs.bytes + h->bufA.bytes + h->bufB.bytes + h->out.bytes;
     for (auto& l : h->lift) b += l.bytes;
-    b += h->tx.tw.bytes + h->tx.cs.bytes + h->tx.eig.bytes + h->ty.tw.bytes + h->ty.cs.bytes + h->ty.eig.bytes;
+    for (const DirTables* t : {&h->tx, &h->ty})
+        b += t->tw.bytes + t->cs.bytes + t->eig.bytes + t->twf.bytes + t->csf.bytes;
+    b += h->psum.bytes + h->zero1.bytes + h->mgstats.bytes + h->zmean.bytes;
     *bytes = b;
     return PP_SUCCESS;
 }
@@ -1341,6 +1345,7 @@ int pp_get_tuning(pp_handle h, pp_tuning* t)
 {
     if (!h) return PP_INVALID_HANDLE;
     if (!t) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
     *t = h->tune;
     return PP_SUCCESS;
 }
