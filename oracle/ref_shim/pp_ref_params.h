@@ -12,13 +12,18 @@
  *   NITER       10 -> 1
  *   RUNINFO      1 -> 0
  * SOLUTIONMETHOD (z-solver: 0 Thomas, 1 PCR, 2 CR-P) can be chosen with
- * -DPP_REF_SOLUTIONMETHOD=<n>; the default is the shipped 0.
+ * -DPP_REF_SOLUTIONMETHOD=<n>, and ZERO_MEAN (subtract the mean of the
+ * solution's real part after the solve) with -DPP_REF_ZERO_MEAN=1; the
+ * defaults are the shipped 0.
  */
 #ifndef _PARAMS_H_
 #define _PARAMS_H_
 
 #ifndef PP_REF_SOLUTIONMETHOD
 #define PP_REF_SOLUTIONMETHOD 0
+#endif
+#ifndef PP_REF_ZERO_MEAN
+#define PP_REF_ZERO_MEAN 0
 #endif
 
 #define PITTPACKACC _OPENACC
@@ -67,7 +72,7 @@ enum PittPackParams {
     PROFILE_COMM = 0,
     NITER = 1,
     RUNINFO = 0,
-    ZERO_MEAN = 0,
+    ZERO_MEAN = PP_REF_ZERO_MEAN,
 };
 
 struct PittPackInputStruct {

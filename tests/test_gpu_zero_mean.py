@@ -5,11 +5,39 @@ solve minus its own mean, for a pure-Neumann (singular, zero-mean RHS) and a
 Dirichlet problem, in FP64 and in the refined mode.  The mean is summed in
 a fixed order, so repeated FP64 solves give the same bits; the refined mode's
 plane sums are accumulated with one atomic per CTA, so its repeats agree to
-round-off."""
+round-off.  The golden files under tests/golden/zero_mean/ pin it to the
+reference's own ZERO_MEAN build."""
+import glob
+import os
+
 import numpy as np
 import pytest
 
+from oracle import oracle as O
+
 pytestmark = pytest.mark.gpu
+
+GOLDEN_ZM = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "zero_mean", "*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN_ZM, ids=[os.path.basename(p)[:-4] for p in GOLDEN_ZM])
+def test_zero_mean_matches_reference_zero_mean_golden(path):
+    """Default options (the reference's zero-mode row replacement) plus
+    zero_mean, against the reference built with ZERO_MEAN on: relative L2
+    <= 1e-12, the plain path's bar."""
+    import pittpack_b200 as pp
+
+    z = np.load(path)
+    nx, ny, nz = int(z["nx"]), int(z["ny"]), int(z["nz"])
+    f = z["f_re"] + 1j * z["f_im"] if z["f_im"].size else z["f_re"]
+    with pp.make_Poisson(nx, ny, nz) as M:
+        M.assignBoundary(str(z["bc"]))
+        M.setBox(tuple(z["box"]))
+        M.setOptions(zero_mean=1)
+        M.assignRhs(f)
+        M.pittPack()
+        P = M.getSolution()
+    assert O.rel_l2(P, z["P"]) <= 1e-12
 
 
 @pytest.mark.parametrize("bc", ["NNNNNN", "DDNNDD", "PPPPNN"])

@@ -9,6 +9,8 @@ import pytest
 from oracle import oracle as O
 
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+# recorded from the reference built with ZERO_MEAN on (tests/golden/make_golden.py)
+GOLDEN_ZM = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "zero_mean", "*.npz")))
 
 
 def _load(path):
@@ -105,3 +107,14 @@ def test_oracle_zero_mean_subtracts_the_solution_mean():
     P1 = O.solve(O.problem(nx, ny, nz, bc, compat_zero_mode=0, zero_mean=1), f)
     assert np.allclose(P1.real, P0.real - P0.real.mean(), rtol=0, atol=1e-14 * np.abs(P0.real).max())
     assert abs(P1.real.mean()) <= 1e-14 * np.abs(P0.real).max()
+
+
+@pytest.mark.parametrize("path", GOLDEN_ZM, ids=[os.path.basename(p)[:-4] for p in GOLDEN_ZM])
+def test_oracle_zero_mean_matches_reference_zero_mean_golden(path):
+    # the reference's subtractMeanValue (src/pencilDcmp.cpp:5649-5683) after
+    # its default solve, against the oracle's zero_mean step
+    nx, ny, nz, bc, box, fr, fi, P = _load(path)
+    Q = O.solve(O.problem(nx, ny, nz, bc, box, zero_mean=1), fr, fi)
+    assert O.rel_l2(Q, P) <= 1e-14
+    assert abs(P.real.mean()) <= 1e-15 * np.abs(P.real).max()
+    assert abs(Q.real.mean()) <= 1e-15 * np.abs(Q.real).max()
