@@ -52,6 +52,20 @@ class PoissonB200 {
     void assignBoundary(const char* bc) { check(pp_assign_boundary(h_, bc), "assignBoundary"); }
     void setBox(const double X[6]) { check(pp_set_box(h_, X), "setBox"); }
     void setCoords(int /*dir*/) {}  // one rank owns the whole box
+    // the reference's MPI neighbourhood and graph set-up: nothing at one rank
+    int constructConnectivity() { return PP_SUCCESS; }
+    void graphCreate() {}
+    // the reference opens and closes PittPack.in without reading it
+    void readIn() {}
+    // the reference's analytic RHS, -4 pi^2 cos(2 pi z) at the cell centres
+    // (src/pencilDcmp.cpp:5685-5759): nx*ny*nz doubles
+    void fillTrigonometric(double* rhs) { check(pp_fill_trigonometric(h_, rhs), "fillTrigonometric"); }
+    // the reference's HDF5 writer is not part of this library: read P with
+    // getSolution() and write it with the caller's own tools
+    void IO(int /*app*/, int /*dir*/, int /*aligndir*/)
+    {
+        throw Error(PP_UNSUPPORTED, "IO: HDF5 output is not provided; read P with getSolution()");
+    }
     void setOptions(const pp_options& o) { check(pp_set_options(h_, &o), "setOptions"); }
     pp_options options() const
     {

@@ -165,6 +165,13 @@ int pp_get_solution_async(pp_handle h, double* P);
 /* getError (src/pencilDcmp.cpp:2040-2208): RMS error of the solution against
  * the reference's manufactured solution; does not modify the solution */
 int pp_get_error_manufactured(pp_handle h, double* err);
+/* fillTrigonometric (src/pencilDcmp.cpp:5685-5759, called by src/main.cpp:115
+ * before assignRhs): the reference's analytic RHS f = -4 pi^2 cos(2 pi z) at
+ * the cell centres z = Za + (k + 1/2) dz of the handle's box, written to rhs
+ * (nx*ny*nz doubles, x fastest).  Host only.  The _box form takes the sizes
+ * and box directly and needs neither a handle nor a GPU. */
+int pp_fill_trigonometric(pp_handle h, double* rhs);
+int pp_fill_trigonometric_box(int nx, int ny, int nz, const double box[6], double* rhs);
 /* multigrid z solver: the most V-cycles any system of the last solve took,
  * and how many systems stopped at the cycle bound above 1e-10 relative
  * residual (waits for the handle's stream); no counterpart in the reference,

@@ -63,3 +63,22 @@ extern "C" int ppref_solve(int nx, int ny, int nz, const char* bc, const double*
     if (seconds) *seconds = M->seconds();
     return 0;
 }
+
+// fillTrigonometric (src/pencilDcmp.cpp:5685-5759) in the order of
+// src/main.cpp:88-115: assignBoundary -> setBox -> setCoords(2) -> fill
+extern "C" int ppref_fill_trigonometric(int nx, int ny, int nz, const char* bc, const double* box, double* rhs)
+{
+    static char arg0[] = "ppref";
+    char* argv[] = {arg0, nullptr};
+    int argc = 1;
+    std::unique_ptr<RefProbe> M(new RefProbe(argc, argv, nx, ny, nz));
+    char mybc[6];
+    std::memcpy(mybc, bc, 6);
+    M->assignBoundary(mybc);
+    double X[6];
+    std::memcpy(X, box, sizeof X);
+    M->setBox(X);
+    M->setCoords(2);
+    M->fillTrigonometric(rhs);
+    return 0;
+}

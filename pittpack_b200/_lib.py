@@ -80,6 +80,8 @@ def load():
         "pp_get_solution_device": ([H, ctypes.c_void_p], i),
         "pp_solution_device_ptr": ([H, ctypes.POINTER(ctypes.c_void_p)], i),
         "pp_get_error_manufactured": ([H, dp], i),
+        "pp_fill_trigonometric": ([H, ctypes.c_void_p], i),
+        "pp_fill_trigonometric_box": ([i, i, i, dp, ctypes.c_void_p], i),
         "pp_zsolve_stats": ([H, ctypes.POINTER(i), ctypes.POINTER(i)], i),
         "pp_set_stream": ([H, ctypes.c_void_p], i),
         "pp_synchronize": ([H], i),

@@ -1,5 +1,6 @@
 // Host side of the solver: plan tables, device buffers, the launch sequence
 // of one solve, and the C ABI declared in include/pittpack_b200.h.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1278,6 +1279,37 @@ int pp_get_error_manufactured(pp_handle h, double* err)
     }
     *err = sqrt(acc / (double)n);
     return PP_SUCCESS;
+}
+
+int pp_fill_trigonometric_box(int nx, int ny, int nz, const double X[6], double* rhs)
+{
+    if (!X || !rhs || nx < 1 || ny < 1 || nz < 1) return PP_INPUT_ARGS;
+    for (int d = 0; d < 3; ++d)
+        if (!(X[2 * d + 1] > X[2 * d]) || !std::isfinite(X[2 * d]) || !std::isfinite(X[2 * d + 1]))
+            return PP_INPUT_ARGS;
+    // the reference's SHIFT = 1 branch: cell centres with the cell size
+    // dxyz[2] of setDxyz (src/pencilDcmp.cpp:828-830) and pi = 4 atan(1)
+    const double pi = 4. * atan(1.0);
+    const double c3 = -(X[4] - X[5]) / (nz);
+    const double shift = 1.0;
+    const size_t plane = (size_t)nx * ny;
+    for (int k = 0; k < nz; ++k) {
+        const double z = X[4] + k * c3 + shift * c3 * 0.5;
+        const double v = -4. * pi * pi * cos(2. * pi * z);
+        std::fill(rhs + plane * k, rhs + plane * (k + 1), v);
+    }
+    return PP_SUCCESS;
+}
+
+int pp_fill_trigonometric(pp_handle h, double* rhs)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    double box[6];
+    {
+        std::lock_guard<std::mutex> g(h->mu);
+        std::memcpy(box, h->box, sizeof box);
+    }
+    return pp_fill_trigonometric_box(h->nx, h->ny, h->nz, box, rhs);
 }
 
 int pp_set_stream(pp_handle h, void* stream)

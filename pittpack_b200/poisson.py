@@ -72,6 +72,39 @@ class PoissonGPU:
     def setCoords(self, dir: int = 2) -> None:  # noqa: A002 - the reference's name
         """Single rank: the rank's box is the whole box; nothing to do."""
 
+    def constructConnectivity(self) -> int:
+        """The reference's MPI neighbourhood set-up
+        (src/pencilDcmp.cpp:851): nothing to connect at one rank."""
+        return _lib.PP_SUCCESS
+
+    def graphCreate(self) -> None:
+        """The reference's MPI graph communicators (src/pencilDcmp.cpp:1274):
+        none at one rank."""
+
+    def readIn(self) -> None:
+        """The reference opens and closes PittPack.in without reading it
+        (src/pencilDcmp.cpp:5790-5796); nothing to do."""
+
+    def fillTrigonometric(self, rhs: np.ndarray | None = None) -> np.ndarray:
+        """The reference's analytic RHS (src/pencilDcmp.cpp:5685-5759):
+        f = -4 pi^2 cos(2 pi z) at the cell centres of the box, shape
+        (nz, ny, nx); fills 'rhs' (contiguous float64) when given."""
+        if rhs is None:
+            rhs = np.empty((self.nz, self.ny, self.nx))
+        if not (isinstance(rhs, np.ndarray) and rhs.dtype == np.float64 and rhs.flags.c_contiguous
+                and rhs.size == self.nx * self.ny * self.nz):
+            raise PittPackError(_lib.PP_INPUT_ARGS, "fillTrigonometric needs a contiguous float64 array of nx*ny*nz")
+        box = np.ascontiguousarray(self._box, dtype=np.float64)
+        check(self._L.pp_fill_trigonometric_box(self.nx, self.ny, self.nz,
+                                                box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rhs.ctypes.data),
+              "fillTrigonometric")
+        return rhs
+
+    def IO(self, app: int = 1, dir: int = 2, aligndir: int = 0) -> None:  # noqa: A002 - the reference's names
+        """The reference's HDF5/XDMF writer (src/pencilDcmp.cpp:1827-1832 ->
+        src/phdf5.cpp) is not part of this library: read P with getSolution()."""
+        raise PittPackError(_lib.PP_UNSUPPORTED, "IO: HDF5 output is not provided; read P with getSolution()")
+
     def options(self) -> Options:
         o = Options()
         check(self._L.pp_get_options(self._h, ctypes.byref(o)), "pp_get_options")

@@ -1,6 +1,8 @@
 """The C++ facade include/PoissonB200.hpp compiles with the usage that
 PittPack's own driver has (make_Poisson -> assignBoundary -> setBox ->
-setCoords -> assignRhs -> pittPack -> getSolution -> getError) and links
+setCoords -> constructConnectivity / graphCreate / readIn ->
+fillTrigonometric -> assignRhs -> pittPack -> getSolution -> IO -> getError;
+IO must throw UNSUPPORTED) and links
 against the library.  Without a GPU the run must end in a thrown
 pittpack_b200::Error carrying a status code, never in a crash; with one it
 solves and prints the manufactured-solution error."""
@@ -28,6 +30,10 @@ int main() {
         double X[6] = {0, 1.0, 0, 1.0, 0, 1.0};
         M->setBox(X);
         M->setCoords(2);
+        M->constructConnectivity();
+        M->graphCreate();
+        M->readIn();
+        M->fillTrigonometric(rhs.data());  // the reference driver's RHS
         pp_options o = M->options();
         o.zero_mean = 1;
         M->setOptions(o);
@@ -37,6 +43,12 @@ int main() {
         M->pittPack();
         std::vector<double> P(2 * Nx * Ny * Nz);
         M->getSolution(P.data());
+        try {
+            M->IO(1, 2, 0);  // the HDF5 writer is not provided: must throw
+            return 4;
+        } catch (const pittpack_b200::Error& e) {
+            if (e.code() != PP_UNSUPPORTED) return 5;
+        }
         std::printf("solved err=%g\n", M->getError());
         return 0;
     } catch (const pittpack_b200::Error& e) {
