@@ -1226,6 +1226,7 @@ int pp_solution_device_ptr(pp_handle h, const double** d_P)
 {
     if (!h) return PP_INVALID_HANDLE;
     if (!d_P) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
     *d_P = h->ext_out ? h->ext_out : h->out.as<double>();
     return PP_SUCCESS;
 }
@@ -1234,7 +1235,14 @@ int pp_get_error_manufactured(pp_handle h, double* err)
 {
     if (!h) return PP_INVALID_HANDLE;
     if (!err) return PP_INPUT_ARGS;
-    if (!h->have_bc) return PP_NOT_READY;
+    double box[6];
+    char bc[6];
+    {
+        std::lock_guard<std::mutex> g(h->mu);
+        if (!h->have_bc) return PP_NOT_READY;
+        std::memcpy(box, h->box, sizeof box);
+        std::memcpy(bc, h->bc, sizeof bc);
+    }
     const int nx = h->nx, ny = h->ny, nz = h->nz;
     const size_t n = (size_t)nx * ny * nz;
     std::vector<double> P(2 * n);
@@ -1242,16 +1250,16 @@ int pp_get_error_manufactured(pp_handle h, double* err)
     if (rc != PP_SUCCESS) return rc;
     // getError (src/pencilDcmp.cpp:2040-2208), INITANALYTIC = 1 branch
     const double pi = REF_PI;
-    const double Xa = h->box[0], Ya = h->box[2], Za = h->box[4];
-    const double c1 = -(h->box[0] - h->box[1]) / (nx);
-    const double c2 = -(h->box[2] - h->box[3]) / (ny);
-    const double c3 = -(h->box[4] - h->box[5]) / (nz);
+    const double Xa = box[0], Ya = box[2], Za = box[4];
+    const double c1 = -(box[0] - box[1]) / (nx);
+    const double c2 = -(box[2] - box[3]) / (ny);
+    const double c3 = -(box[4] - box[5]) / (nz);
     const double omega[3] = {1 * pi, 2 * pi, 3 * pi};
-    const int t0 = ref_tag_xy(kind_from_bc(h->bc[0], h->bc[1]));
-    const int t1 = ref_tag_xy(kind_from_bc(h->bc[2], h->bc[3]));
-    const int t2 = ref_tag_z(h->bc);
-    const bool pxy = h->bc[0] == 'P' || h->bc[2] == 'P';
-    const bool pall = h->bc[0] == 'P' && h->bc[2] == 'P' && h->bc[4] == 'P';
+    const int t0 = ref_tag_xy(kind_from_bc(bc[0], bc[1]));
+    const int t1 = ref_tag_xy(kind_from_bc(bc[2], bc[3]));
+    const int t2 = ref_tag_z(bc);
+    const bool pxy = bc[0] == 'P' || bc[2] == 'P';
+    const bool pall = bc[0] == 'P' && bc[2] == 'P' && bc[4] == 'P';
     double acc = 0.0;
     for (int k = 0; k < nz; ++k) {
         const double z = Za + k * c3 + 1.0 * c3 * 0.5;
@@ -1408,14 +1416,18 @@ int pp_autotune(pp_handle h, int reps, pp_tuning* chosen, double* best_ms)
 {
     if (!h) return PP_INVALID_HANDLE;
     if (reps < 1 || reps > 100) return PP_INPUT_ARGS;
-    if (!h->have_bc || !h->have_rhs) return PP_NOT_READY;
+    pp_tuning start;
+    {
+        std::lock_guard<std::mutex> g(h->mu);
+        if (!h->have_bc || !h->have_rhs) return PP_NOT_READY;
+        start = h->tune;
+    }
     cudaSetDevice(h->device);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         if (e0) cudaEventDestroy(e0);
         return PP_CUDA_ERROR;
     }
-    const pp_tuning start = h->tune;
     pp_tuning best{0, 0, 0};
     double bms = 0.0;
     int rc = time_config(h, best, reps, e0, e1, &bms);
