@@ -1400,14 +1400,14 @@ static int time_config(pp_handle h, const pp_tuning& t, int reps, cudaEvent_t e0
     }
     int rc = pp_solve(h);
     if (rc != PP_SUCCESS) return rc;
-    cudaEventRecord(e0, h->stream);
+    cudaError_t e = cudaEventRecord(e0, h->stream);
+    if (e != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
     for (int r = 0; r < reps && rc == PP_SUCCESS; ++r) rc = pp_solve(h);
-    cudaEventRecord(e1, h->stream);
     if (rc != PP_SUCCESS) return rc;
-    cudaError_t e = cudaEventSynchronize(e1);
+    if ((e = cudaEventRecord(e1, h->stream)) == cudaSuccess) e = cudaEventSynchronize(e1);
     if (e != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
     float f = 0.f;
-    cudaEventElapsedTime(&f, e0, e1);
+    if ((e = cudaEventElapsedTime(&f, e0, e1)) != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
     *ms = f / reps;
     return PP_SUCCESS;
 }
