@@ -118,3 +118,35 @@ def test_oracle_zero_mean_matches_reference_zero_mean_golden(path):
     assert O.rel_l2(Q, P) <= 1e-14
     assert abs(P.real.mean()) <= 1e-15 * np.abs(P.real).max()
     assert abs(Q.real.mean()) <= 1e-15 * np.abs(Q.real).max()
+
+
+REF_LIB = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "libppref.so")
+SWEEP = [fx + fy + z for fx in ("PP", "NN", "DD") for fy in ("PP", "NN", "DD") for z in ("DD", "NN", "DN", "ND", "PP")]
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference build absent (make -C oracle)")
+@pytest.mark.parametrize("bc", SWEEP)
+def test_oracle_equals_the_reference_build_on_every_family(bc):
+    """Live sweep against the reference's own CPU solve (oracle/_ref): every
+    x/y family pair the reference has times every z end pair, two shapes
+    (odd and even lengths), a non-unit box, RHS as given (no compatibility
+    projection for the singular sets), complex data when x is periodic."""
+    import ctypes
+
+    L = ctypes.CDLL(REF_LIB)
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.ppref_solve.argtypes = [ctypes.c_int] * 3 + [ctypes.c_char_p, dp, dp, dp, dp, dp]
+    L.ppref_solve.restype = ctypes.c_int
+    box = np.array([0, 1, 0, 2, -1, 1.0])
+    for k, (nx, ny, nz) in enumerate([(8, 6, 5), (10, 12, 9)]):
+        rng = np.random.default_rng(SWEEP.index(bc) * 2 + k)
+        fr = rng.uniform(-1, 1, (nz, ny, nx))
+        fi = rng.uniform(-1, 1, (nz, ny, nx)) if bc[0] == "P" else None
+        out = np.zeros(2 * nx * ny * nz)
+        sec = ctypes.c_double()
+        rc = L.ppref_solve(nx, ny, nz, bc.encode(), box.ctypes.data_as(dp), fr.ctypes.data_as(dp),
+                           None if fi is None else fi.ctypes.data_as(dp), out.ctypes.data_as(dp), ctypes.byref(sec))
+        assert rc == 0
+        Q = O.solve(O.problem(nx, ny, nz, bc, tuple(box)), fr, fi)
+        # identical bits on this image; the bound allows another libm
+        assert O.rel_l2(Q, out.view(np.complex128).reshape(nz, ny, nx)) <= 1e-15, (bc, (nx, ny, nz))
