@@ -102,5 +102,11 @@ inline std::unique_ptr<PoissonB200> make_Poisson(int nx, int ny, int nz)
 {
     return std::unique_ptr<PoissonB200>(new PoissonB200(nx, ny, nz));
 }
+// with the reference's signature: argc / argv only fed MPI_Init there
+// (src/pencilDcmp.cpp:232-452); one rank needs neither
+inline std::unique_ptr<PoissonB200> make_Poisson(int /*argc*/, char** /*argv*/, int nx, int ny, int nz)
+{
+    return make_Poisson(nx, ny, nz);
+}
 
 }  // namespace pittpack_b200

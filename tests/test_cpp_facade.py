@@ -20,11 +20,12 @@ SRC = r'''
 #include <vector>
 #include "PoissonB200.hpp"
 
-int main() {
+int main(int argc, char* argv[]) {
     const int Nx = 16, Ny = 16, Nz = 8;
     std::vector<double> rhs(Nx * Ny * Nz, 1.0);
     try {
-        auto M = pittpack_b200::make_Poisson(Nx, Ny, Nz);
+        using pittpack_b200::make_Poisson;
+        auto M = make_Poisson(argc, argv, Nx, Ny, Nz);  // the reference's call
         char mybc[6] = {'N', 'N', 'N', 'N', 'D', 'D'};
         M->assignBoundary(mybc);
         double X[6] = {0, 1.0, 0, 1.0, 0, 1.0};
