@@ -1,8 +1,10 @@
 // PoissonB200.hpp -- header-only C++ facade over include/pittpack_b200.h with
 // the method names of PittPack's PencilDcmp (src/include/pencilDcmp.hpp:442-466),
-// so a driver written like src/main.cpp needs only a different factory:
+// so a driver written like src/main.cpp needs only the factory from this
+// namespace (the same call):
 //
-//     auto M = pittpack_b200::make_Poisson(nx, ny, nz);
+//     using pittpack_b200::make_Poisson;
+//     auto M = make_Poisson(argc, argv, nx, ny, nz);
 //     char bc[6] = {'N','N','N','N','D','D'};
 //     M->assignBoundary(bc);
 //     double X[6] = {0, 1, 0, 1, 0, 1};
