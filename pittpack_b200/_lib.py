@@ -1,7 +1,7 @@
 """ctypes binding of libpittpack_b200.so (the C ABI in include/pittpack_b200.h).
 
-The product path: if the library is missing the import fails loudly; there is
-no CPU fallback.
+The product path: if the library is missing, the first call that needs it
+raises ImportError with the build command; there is no CPU fallback.
 """
 from __future__ import annotations
 
