@@ -67,3 +67,12 @@ def test_server_submit_checks_host_buffers():
     with pytest.raises(ValueError):
         S.submit(4, 4, 4, "NNNNDD", np.zeros(n), np.zeros(n, dtype=np.float64))
     assert S._keep == {}
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """No CPU fallback: without libpittpack_b200.so the first call raises
+    ImportError naming the build command."""
+    monkeypatch.setattr(_lib, "_lib", None)
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "libpittpack_b200.so"))
+    with pytest.raises(ImportError, match="pittpack_b200.build"):
+        PoissonGPU(8, 8, 8)
