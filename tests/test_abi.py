@@ -66,3 +66,24 @@ def test_no_gpu_here_reports_init_failure(lib):
 
     h = ctypes.c_void_p()
     assert _lib.load().pp_create(8, 8, 8, ctypes.byref(h)) == 1  # GPU_INIT_FAILURE
+
+
+@pytest.mark.skipif(not __import__("shutil").which("gcc"), reason="no C compiler")
+def test_header_is_plain_c_and_links(tmp_path):
+    """The ABI is C: a C99 translation unit that includes the header and
+    takes the address of every declared entry point compiles, with no CUDA
+    headers, and links against the library."""
+    import subprocess
+
+    names = _declared()
+    src = tmp_path / "abi.c"
+    src.write_text('#include "pittpack_b200.h"\n#include <stdio.h>\nint main(void) {\n'
+                   "    const void* fns[] = {\n" + ",\n".join(f"        (const void*){n}" for n in names) + "\n    };\n"
+                   '    printf("%d %s\\n", (int)(sizeof fns / sizeof fns[0]), pp_result_string(PP_INPUT_ARGS));\n'
+                   "    return 0;\n}\n")
+    libdir = os.path.join(ROOT, "pittpack_b200")
+    exe = tmp_path / "abi"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-L", libdir,
+                    "-lpittpack_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split(maxsplit=1)
+    assert int(out[0]) == len(names) and out[1].startswith("INPUT_ARGS")
