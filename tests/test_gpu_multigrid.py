@@ -1,7 +1,9 @@
-"""The multigrid alternate z solver gives the default direct solve's answer:
-both solve the same z systems, the V-cycles down to the FP64 rounding floor.
-Tolerance: relative L2 <= 1e-10 against the direct path, with no system left
-at the cycle bound."""
+"""The multigrid alternate z solver (the reference's MultiGrid, src/multiGrid.cpp:
+1105-1515, reached through PencilDcmp::solveMG, src/pencilDcmp.cpp:4047-4135)
+solves the same z systems as the direct path, its V-cycles down to the FP64
+rounding floor.  Tolerance: relative L2 <= 1e-10 against the CPU oracle
+(oracle/pp_oracle.c, the reference's Thomas solve restated) and against the
+direct path, with no system left at the cycle bound."""
 import numpy as np
 import pytest
 
@@ -43,6 +45,23 @@ def test_multigrid_matches_direct(bc, shape, compat):
     assert _rel(P, Q) <= TOL
     assert stuck == 0
     assert cycles <= 40
+
+
+@pytest.mark.parametrize("bc", CASES)
+@pytest.mark.parametrize("shape", [(32, 16, 64), (20, 12, 100)])
+@pytest.mark.parametrize("compat", [1, 0])
+def test_multigrid_matches_oracle(bc, shape, compat):
+    from oracle import oracle as O
+
+    nx, ny, nz = shape
+    rng = np.random.default_rng(nz * 11 + len(bc))
+    f = rng.standard_normal((nz, ny, nx))
+    if all(bc[k:k + 2] in ("PP", "NN") for k in (0, 2, 4)):
+        f -= f.mean()
+    Q = O.solve(O.problem(nx, ny, nz, bc, compat_zero_mode=compat), f)
+    P, (cycles, stuck) = _solve(nx, ny, nz, bc, f, compat_zero_mode=compat, z_solver=1)
+    assert _rel(P, Q) <= TOL
+    assert stuck == 0
 
 
 def test_multigrid_larger_grid():
