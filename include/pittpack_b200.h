@@ -248,25 +248,33 @@ int pp_server_submit(pp_server s, const pp_request* r, unsigned long long* ticke
 int pp_server_wait(pp_server s, unsigned long long ticket, double* latency_ms, int* precision);
 /* requests completed, most requests on the GPU at once, bytes of pooled handles */
 int pp_server_stats(pp_server s, long long* completed, int* max_inflight, size_t* pool_bytes);
+/* pooled handles created and evicted so far (each creation allocates device
+ * memory, each eviction frees it) */
+int pp_server_pool_stats(pp_server s, long long* created, long long* evicted);
 /* finishes queued requests, then frees everything */
 int pp_server_destroy(pp_server s);
 
 /* pp_solve_noalloc -- no counterpart in the reference.  One plain FP64 solve
  * (the reference's semantics and default options, like pp_solve) that
- * allocates no device memory, for callers that cannot call cudaMalloc: code
- * running inside host callbacks or allocator-restricted services, plugins that
- * must not grow the device heap of their host process, callers whose own
- * allocator owns all device memory.  The caller passes device pointers: d_rhs
- * (real RHS, nx*ny*nz doubles, x fastest) and d_P (the solution, 2*nx*ny*nz
- * doubles, chunkedArray layout); 'stream' is a cudaStream_t (0 = legacy) and
- * the call returns once the work is enqueued.  The spectra and tables live in
- * one fixed 32 MiB device array inside the library (held by every GPU that
- * loads it until exit): about 16 bytes per point for the real families and
- * 32 bytes per point when x or y is periodic, so up to ~2 M and ~1 M points;
- * larger grids return PP_NOALLOC_TOO_LARGE.  All calls share that array: calls
- * that overlap on the GPU race, so serialise them on one stream.  The first
- * call on a device looks up the array's device address; make it before any
- * stream capture. */
+ * allocates no device memory, for callers that cannot call cudaMalloc: a
+ * service whose device memory all belongs to its own pool allocator, a plugin
+ * that must not grow the device heap of the process that loads it, any
+ * allocation-restricted context that still owns its input and output
+ * buffers.  The caller passes device pointers: d_rhs (real RHS, nx*ny*nz
+ * doubles, x fastest) and d_P (the solution, 2*nx*ny*nz doubles,
+ * chunkedArray layout); 'stream' is a cudaStream_t (0 = legacy).  The tables
+ * are computed on the device, nothing is copied from the host, and the call
+ * returns once its kernels are enqueued on 'stream'.  The spectra and tables
+ * live in one fixed 32 MiB device array inside the library (held by every GPU
+ * that loads it until exit): about 16 bytes per point for the real families
+ * and 32 bytes per point when x or y is periodic, so up to ~2 M and ~1 M
+ * points; larger grids return PP_NOALLOC_TOO_LARGE before anything is
+ * launched.  All calls share that array and it keeps the last call's
+ * contents (each call writes everything it reads): calls that overlap on the
+ * GPU race, so serialise them on one stream.  The first call on a device
+ * looks up the array's device address; make it before any stream capture.
+ * Like any call that launches work it must not be made from a stream
+ * callback (cudaLaunchHostFunc), where CUDA forbids CUDA calls. */
 int pp_solve_noalloc(int nx, int ny, int nz, const char bc[6], const double box[6], const double* d_rhs,
                      double* d_P, void* stream);
 

@@ -56,9 +56,10 @@ def _bind(L):
     L.pp_server_wait.argtypes = [H, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i)]
     L.pp_server_stats.argtypes = [H, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(i),
                                   ctypes.POINTER(ctypes.c_size_t)]
+    L.pp_server_pool_stats.argtypes = [H, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     L.pp_server_destroy.argtypes = [H]
     for n in ("pp_batch_create", "pp_batch_run", "pp_batch_info", "pp_batch_destroy", "pp_server_create",
-              "pp_server_submit", "pp_server_wait", "pp_server_stats", "pp_server_destroy"):
+              "pp_server_submit", "pp_server_wait", "pp_server_stats", "pp_server_pool_stats", "pp_server_destroy"):
         getattr(L, n).restype = i
     L._pp_batch_bound = True
     return L
@@ -156,7 +157,10 @@ class Server:
     def stats(self):
         c, m, b = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_size_t()
         check(self._L.pp_server_stats(self._h, ctypes.byref(c), ctypes.byref(m), ctypes.byref(b)), "pp_server_stats")
-        return {"completed": c.value, "max_inflight": m.value, "pool_bytes": b.value}
+        cr, ev = ctypes.c_longlong(), ctypes.c_longlong()
+        check(self._L.pp_server_pool_stats(self._h, ctypes.byref(cr), ctypes.byref(ev)), "pp_server_pool_stats")
+        return {"completed": c.value, "max_inflight": m.value, "pool_bytes": b.value,
+                "handles_created": cr.value, "handles_evicted": ev.value}
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

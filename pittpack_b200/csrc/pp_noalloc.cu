@@ -1,13 +1,16 @@
 // pp_solve_noalloc: the plain FP64 solve for callers that cannot allocate
 // device memory.
 //
-// Who needs it: code that runs where cudaMalloc is not an option -- inside a
-// host callback or a memory-pool-restricted service, a plugin that must not
-// grow the device heap of the process that loads it, or a caller whose own
-// allocator owns all device memory.  Those callers can still hand over their
-// RHS and solution buffers; everything else the solve needs (the two spectral
-// workspaces and the twiddle / eigenvalue / boundary tables) lives in one
-// fixed file-scope device array instead of being allocated per handle.
+// Who needs it: code that runs where cudaMalloc is not an option -- a service
+// whose device memory is all owned by its own pool allocator, a plugin that
+// must not grow the device heap of the process that loads it, or an
+// allocation-restricted context that still owns its input and output
+// buffers.  Those callers hand over their RHS and solution buffers;
+// everything else the solve needs (the two spectral workspaces and the
+// twiddle / eigenvalue / boundary tables) lives in one fixed file-scope
+// device array instead of being allocated per handle, and the tables are
+// computed on the device by a small kernel, so the call copies nothing from
+// the host and returns once its kernels are enqueued.
 //
 // Limits and sharing:
 //   * the array is PP_NOALLOC_SCRATCH_BYTES (32 MiB); every GPU that loads the
@@ -21,22 +24,24 @@
 //     threads) race on the array: serialise them on one stream;
 //   * the first call on a device resolves the array's device address with
 //     cudaGetSymbolAddress (that device current) and caches it; make that first
-//     call before any stream capture.
+//     call before any stream capture;
+//   * like every call that launches work, it must not be made from a stream
+//     callback (cudaLaunchHostFunc / cudaStreamAddCallback), where CUDA
+//     forbids CUDA calls.
+#include <algorithm>
 #include <cmath>
 #include <mutex>
-#include <vector>
 
 #include "../../include/pittpack_b200.h"
 #include "pp_common.cuh"
 #include "pp_kernels.h"
+#include "pp_tables.cuh"
 
 #define PP_NOALLOC_SCRATCH_BYTES (32u << 20)
 
 static __device__ __align__(256) unsigned char pp_noalloc_scratch[PP_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-
-const double NA_PI = 3.1415926535897932384;  // the reference's pi constant
 
 std::mutex g_mu;
 void* g_scratch[128];  // device address of the array, per device
@@ -80,12 +85,10 @@ bool na_radix(int n, PPFftPlan& P)
     return m == 1;
 }
 
-// host copies of one direction's tables (the same values the handle path uploads)
+// one direction of the solve: its length, family and FFT plan
 struct NaDir {
-    int n = 0, kind = -1;
+    int n = 0, nf = 0, kind = -1;
     PPFftPlan fft{};
-    std::vector<double2> tw, cs;
-    std::vector<double> eig;
 };
 
 int na_dir(NaDir& d, int n, int kind)
@@ -94,46 +97,8 @@ int na_dir(NaDir& d, int n, int kind)
     d.kind = kind;
     const bool quarter = pp_kind_is_quarter(kind);
     if (quarter && n % 2) return PP_UNSUPPORTED;
-    const int nf = quarter ? n / 2 : n;
-    if (!na_radix(nf, d.fft)) return PP_UNSUPPORTED;
-    const long double two_pi = 6.283185307179586476925286766559005768L;
-    const long double pi_l = 3.141592653589793238462643383279502884L;
-    d.tw.resize(nf);
-    for (int m = 0; m < nf; ++m) {
-        const long double a = -two_pi * (long double)m / (long double)nf;
-        d.tw[m] = make_double2((double)cosl(a), (double)sinl(a));
-    }
-    d.cs.resize(n);
-    if (quarter) {
-        for (int m = 0; m < nf; ++m) {
-            const long double a = -pi_l * (long double)m / (long double)n;
-            d.cs[m] = make_double2((double)cosl(a), (double)sinl(a));
-        }
-        for (int p = 0; p < nf; ++p) {
-            const long double a = -pi_l * (long double)(4 * p + 1) / (4.0L * n);
-            d.cs[nf + p] = make_double2((double)cosl(a), (double)sinl(a));
-        }
-    } else {
-        for (int k = 0; k < n; ++k) {
-            const double theta = (NA_PI / 2. / n) * k;
-            d.cs[k] = make_double2(cos(theta), sin(theta));
-        }
-    }
-    double num = 0.0, freq = NA_PI;
-    if (kind == PP_KIND_DST2) num = 1.0;
-    else if (kind == PP_KIND_FFT) freq = 2. * NA_PI;
-    else if (quarter) num = 0.5;
-    d.eig.resize(n);
-    for (int k = 0; k < n; ++k) d.eig[k] = -2.0 + 2. * cos((k + num) * freq / (n + 0.0));
-    return PP_SUCCESS;
-}
-
-double na_exact(double omega, double x, int tg)
-{
-    if (fabs(omega) < 1.0e-6) return 1.0;
-    if (tg == 0 || tg == -1 || tg == -2) return sin(omega * x);
-    if (tg == 1) return cos(omega * x);
-    return 0.0;
+    d.nf = quarter ? n / 2 : n;
+    return na_radix(d.nf, d.fft) ? PP_SUCCESS : PP_UNSUPPORTED;
 }
 
 int na_tag_xy(int kind) { return kind == PP_KIND_DST2 ? 0 : kind == PP_KIND_DCT2 ? 1 : kind == PP_KIND_FFT ? 2 : -1; }
@@ -155,6 +120,79 @@ int na_tag_z(const char* bc)
     if (bc[4] == 'D') return -1;
     if (bc[4] == 'N') return -2;
     return t[2];
+}
+
+// The tables of one call, written by one kernel into the scratch array:
+// segments 0-2 / 3-5 are the FFT twiddles, family twiddles and eigenvalue
+// parts of x / y, 6-11 the manufactured Dirichlet faces (slots 0-5, null
+// where the face is not subtracted).  Values: the handle path's formulas
+// (pp_tables.cuh); the FFT twiddles e^{-2 pi i m / nf} through sincospi.
+struct NaTables {
+    double2* tw[2];
+    double2* cs[2];
+    double* eig[2];
+    double* face[6];
+    int n[2], nf[2], kind[2];
+    long len[12];
+    PPMmsFaces mp;
+};
+
+__global__ void na_tables_kernel(NaTables t)
+{
+    long total = 0;
+    for (int s = 0; s < 12; ++s) total += t.len[s];
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < total; g += (long)gridDim.x * blockDim.x) {
+        long q = g;
+        int s = 0;
+        while (q >= t.len[s]) q -= t.len[s++];
+        const int idx = (int)q;
+        if (s < 6) {
+            const int d = s / 3, part = s % 3;
+            const int n = t.n[d], nf = t.nf[d], kind = t.kind[d];
+            if (part == 0) {
+                double sn, c;
+                sincospi(-2.0 * idx / nf, &sn, &c);
+                t.tw[d][idx] = make_double2(c, sn);
+            } else if (part == 1) {
+                if (pp_kind_is_quarter(kind)) {
+                    double sn, c;
+                    if (idx < nf) sincospi(-(double)idx / n, &sn, &c);
+                    else sincospi(-(double)(4 * (idx - nf) + 1) / (4.0 * n), &sn, &c);
+                    t.cs[d][idx] = make_double2(c, sn);
+                } else {
+                    t.cs[d][idx] = pp_family_twiddle(n, idx);
+                }
+            } else {
+                t.eig[d][idx] = pp_eigen_part(n, kind, idx);
+            }
+        } else {
+            const int slot = s - 6;
+            int na, nb;
+            pp_mms_face_dims(t.mp, slot, &na, &nb);
+            const int a = idx % na, b = idx / na;
+            t.face[slot][idx] = pp_mms_face_value(t.mp, slot, a, b);
+        }
+    }
+}
+
+// whether a manufactured face has a nonzero value: its values are
+// 2 A(a) B(b) C, products of O(1) sines and cosines (no underflow), so it is
+// nonzero exactly when each factor is nonzero somewhere; checked on the
+// factors, without forming the face
+bool na_face_nonzero(const PPMmsFaces& p, int slot)
+{
+    auto any = [](int n, auto f) {
+        for (int i = 0; i < n; ++i)
+            if (f(i) != 0.0) return true;
+        return false;
+    };
+    const double w = pp_mms_face_plane(p, slot);
+    auto X = [&](int i) { return pp_exact_value(p.omega[0], pp_mms_x(p, i), p.t0); };
+    auto Y = [&](int j) { return pp_exact_value(p.omega[1], pp_mms_y(p, j), p.t1); };
+    auto Z = [&](int k) { return pp_exact_value(p.omega[2], pp_mms_z(p, k), p.t2); };
+    if (slot < 2) return any(p.nx, X) && any(p.ny, Y) && pp_exact_value(p.omega[2], w, p.t2) != 0.0;
+    if (slot < 4) return pp_exact_value(p.omega[0], w, p.t0) != 0.0 && any(p.ny, Y) && any(p.nz, Z);
+    return any(p.nx, X) && pp_exact_value(p.omega[1], w, p.t1) != 0.0 && any(p.nz, Z);
 }
 
 // a bump allocator over the scratch array (256-byte aligned pieces)
@@ -230,76 +268,59 @@ extern "C" int pp_solve_noalloc(int nx, int ny, int nz, const char bc[6], const 
     Carve cv{static_cast<unsigned char*>(sp)};
     double* A = cv.take<double>(n * ((x_cplx || s_cplx) ? 2 : 1));
     double* B = cv.take<double>(n * (s_cplx ? 2 : 1));
-    double2* twx = cv.take<double2>(tx.tw.size());
-    double2* csx = cv.take<double2>(tx.cs.size());
-    double* eigx = cv.take<double>(nx);
-    double2* twy = cv.take<double2>(ty.tw.size());
-    double2* csy = cv.take<double2>(ty.cs.size());
-    double* eigy = cv.take<double>(ny);
+    NaTables tb{};
+    const NaDir* dirs[2] = {&tx, &ty};
+    for (int d = 0; d < 2; ++d) {
+        tb.n[d] = dirs[d]->n;
+        tb.nf[d] = dirs[d]->nf;
+        tb.kind[d] = dirs[d]->kind;
+        tb.tw[d] = cv.take<double2>(dirs[d]->nf);
+        tb.cs[d] = cv.take<double2>(dirs[d]->n);
+        tb.eig[d] = cv.take<double>(dirs[d]->n);
+        tb.len[3 * d] = dirs[d]->nf;
+        tb.len[3 * d + 1] = dirs[d]->n;
+        tb.len[3 * d + 2] = dirs[d]->n;
+    }
 
-    // Dirichlet face corrections (modifyRhsDirichlet, src/pencilDcmp.cpp:4623-4835)
+    // manufactured Dirichlet faces (modifyRhsDirichlet, src/pencilDcmp.cpp:4623-4835)
+    PPMmsFaces& mp = tb.mp;
+    mp.nx = nx;
+    mp.ny = ny;
+    mp.nz = nz;
     const double pi = 4. * atan(1.0);
-    const double Xa = box[0], Ya = box[2], Za = box[4];
-    const double c1 = -(box[0] - box[1]) / nx, c2 = -(box[2] - box[3]) / ny, c3 = -(box[4] - box[5]) / nz;
-    const double omega[3] = {1 * pi, 2 * pi, 3 * pi};
-    const int t0 = na_tag_xy(kx), t1 = na_tag_xy(ky), t2 = na_tag_z(bc);
-    std::vector<double> face[6];
-    for (int f = 0; f < 2; ++f)
-        if (bc[4 + f] == 'D') {
-            face[f].resize((size_t)nx * ny);
-            const double z = f == 0 ? Za : Za + (nz - 1) * c3 + c3;
-            for (int i = 0; i < nx; ++i)
-                for (int j = 0; j < ny; ++j)
-                    face[f][i + (size_t)nx * j] = 2. * na_exact(omega[0], Xa + i * c1 + c1 * .5, t0) *
-                                                  na_exact(omega[1], Ya + j * c2 + c2 * 0.5, t1) *
-                                                  na_exact(omega[2], z, t2);
-        }
-    for (int f = 0; f < 2; ++f)
-        if (bc[f] == 'D') {
-            face[2 + f].resize((size_t)ny * nz);
-            const double x = f == 0 ? Xa : Xa + nx * c1;
-            for (int k = 0; k < nz; ++k)
-                for (int j = 0; j < ny; ++j)
-                    face[2 + f][j + (size_t)ny * k] = 2. * na_exact(omega[0], x, t0) *
-                                                      na_exact(omega[1], Ya + j * c2 + c2 * 0.5, t1) *
-                                                      na_exact(omega[2], Za + k * c3 + c3 * .5, t2);
-        }
-    for (int f = 0; f < 2; ++f)
-        if (bc[2 + f] == 'D') {
-            face[4 + f].resize((size_t)nx * nz);
-            const double y = f == 0 ? Ya : Ya + ny * c2;
-            for (int k = 0; k < nz; ++k)
-                for (int i = 0; i < nx; ++i)
-                    face[4 + f][i + (size_t)nx * k] = 2. * na_exact(omega[0], Xa + i * c1 + c1 * 0.5, t0) *
-                                                      na_exact(omega[1], y, t1) *
-                                                      na_exact(omega[2], Za + k * c3 + c3 * .5, t2);
-        }
-    double* fdev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    for (int f = 0; f < 6; ++f) {
-        bool nonzero = false;
-        for (double v : face[f]) nonzero |= v != 0.0;
-        if (nonzero) fdev[f] = cv.take<double>(face[f].size());
+    mp.Xa = box[0];
+    mp.Ya = box[2];
+    mp.Za = box[4];
+    mp.c1 = -(box[0] - box[1]) / nx;
+    mp.c2 = -(box[2] - box[3]) / ny;
+    mp.c3 = -(box[4] - box[5]) / nz;
+    mp.omega[0] = 1 * pi;
+    mp.omega[1] = 2 * pi;
+    mp.omega[2] = 3 * pi;
+    mp.t0 = na_tag_xy(kx);
+    mp.t1 = na_tag_xy(ky);
+    mp.t2 = na_tag_z(bc);
+    static const int face_of_slot[6] = {4, 5, 0, 1, 2, 3};  // slot -> xmin, xmax, ymin, ymax, zmin, zmax
+    for (int slot = 0; slot < 6; ++slot) {
+        if (bc[face_of_slot[slot]] != 'D' || !na_face_nonzero(mp, slot)) continue;
+        int na, nb;
+        pp_mms_face_dims(mp, slot, &na, &nb);
+        tb.face[slot] = cv.take<double>((size_t)na * nb);
+        tb.len[6 + slot] = (long)na * nb;
     }
     if (!cv.ok) return PP_NOALLOC_TOO_LARGE;
 
     cudaStream_t st = (cudaStream_t)stream;
-#define PP_NA_UP(dst, vec)                                                                                     \
-    if (cudaMemcpyAsync(dst, (vec).data(), sizeof((vec)[0]) * (vec).size(), cudaMemcpyHostToDevice, st) !=      \
-        cudaSuccess)                                                                                           \
-        return PP_CUDA_ERROR;
-    PP_NA_UP(twx, tx.tw);
-    PP_NA_UP(csx, tx.cs);
-    PP_NA_UP(eigx, tx.eig);
-    PP_NA_UP(twy, ty.tw);
-    PP_NA_UP(csy, ty.cs);
-    PP_NA_UP(eigy, ty.eig);
-    for (int f = 0; f < 6; ++f)
-        if (fdev[f]) {
-            PP_NA_UP(fdev[f], face[f]);
-        }
-#undef PP_NA_UP
-    PPLift lift{fdev[0], fdev[1], fdev[2], fdev[3], fdev[4], fdev[5], 0};
-    lift.any = (fdev[0] || fdev[1] || fdev[2] || fdev[3] || fdev[4] || fdev[5]) ? 1 : 0;
+    long total = 0;
+    for (int q = 0; q < 12; ++q) total += tb.len[q];
+    const int tblocks = (int)std::min<long>((total + 255) / 256, 1184);
+    na_tables_kernel<<<tblocks, 256, 0, st>>>(tb);
+    if (cudaGetLastError() != cudaSuccess) return PP_CUDA_ERROR;
+    PPLift lift{tb.face[0], tb.face[1], tb.face[2], tb.face[3], tb.face[4], tb.face[5], 0};
+    lift.any = (lift.z0 || lift.z1 || lift.x0 || lift.x1 || lift.y0 || lift.y1) ? 1 : 0;
+    const double2 *twx = tb.tw[0], *csx = tb.cs[0], *twy = tb.tw[1], *csy = tb.cs[1];
+    const double *eigx = tb.eig[0], *eigy = tb.eig[1];
+    const double c1 = mp.c1, c2 = mp.c2, c3 = mp.c3;
 
     // the five passes of the solve (as pp_solve, default options)
     const long plane = (long)nx * ny;
@@ -339,7 +360,9 @@ extern "C" int pp_solve_noalloc(int nx, int ny, int nz, const char bc[6], const 
     z.ny = ny;
     z.nz = nz;
     int zthreads = 0;
-    pp_zsolve_config(nz, s_cplx, nx, &z.TS, &zthreads);
+    // the handle path's launch shape for this grid (lanes per system chosen
+    // by the number of systems; the launch derives the same lane count)
+    pp_zsolve_config_p(nz, s_cplx, nx, 0, &z.TS, &zthreads, 0, ny);
     z.tiles_x = (nx + z.TS - 1) / z.TS;
     z.ax = eigx;
     z.ay = eigy;

@@ -67,6 +67,7 @@ struct Slot {
     PooledHandle* ph = nullptr;
     int precision = 0;
     Clock::time_point t_submit;
+    int status = PP_SUCCESS;       // PP_CUDA_ERROR when the completion could not be awaited
     Clock::time_point t_done;      // written by the host function
     std::atomic<int> finished{0};  // set by the host function after t_done
     struct pp_server_s* server = nullptr;
@@ -88,6 +89,7 @@ struct pp_server_s {
     std::thread worker;
     long long n_done = 0;
     int max_inflight = 0;
+    long long n_created = 0, n_evicted = 0;  // pooled handles made / freed
 };
 
 namespace {
@@ -142,6 +144,7 @@ PooledHandle* acquire(pp_server_s* S, const pp_request& r, const ShapeKey& key, 
         S->pool_bytes -= victim->bytes;
         pp_destroy(victim->h);
         S->pool.erase(victim);
+        S->n_evicted++;
     }
     pp_handle h = nullptr;
     if ((*rc = pp_create(r.nx, r.ny, r.nz, &h)) != PP_SUCCESS) return nullptr;
@@ -153,6 +156,7 @@ PooledHandle* acquire(pp_server_s* S, const pp_request& r, const ShapeKey& key, 
     pp_workspace_bytes(h, &bytes);
     S->pool.push_back(PooledHandle{h, key, bytes, Clock::now()});
     S->pool_bytes += bytes;
+    S->n_created++;
     return &S->pool.back();
 }
 
@@ -160,6 +164,7 @@ void retire(pp_server_s* S, Slot& s)
 {
     Result& res = S->results[s.ticket];
     res.done = true;
+    res.status = s.status;
     res.precision = s.precision;
     res.latency_ms = std::chrono::duration<double, std::milli>(s.t_done - s.t_submit).count();
     s.finished.store(0, std::memory_order_relaxed);
@@ -218,8 +223,10 @@ bool admit(pp_server_s* S, const Req& q)
     s.ph = ph;
     s.precision = prec;
     s.t_submit = q.t_submit;
+    s.status = PP_SUCCESS;
     if (cudaLaunchHostFunc(s.stream, on_complete, &s) != cudaSuccess) {
-        cudaStreamSynchronize(s.stream);
+        // no completion callback: wait here, and fail the request if even that fails
+        if (cudaStreamSynchronize(s.stream) != cudaSuccess) s.status = PP_CUDA_ERROR;
         s.t_done = Clock::now();
         s.finished.store(1, std::memory_order_release);
     }
@@ -324,6 +331,15 @@ extern "C" int pp_server_stats(pp_server S, long long* completed, int* max_infli
     if (completed) *completed = S->n_done;
     if (max_inflight) *max_inflight = S->max_inflight;
     if (pool_bytes) *pool_bytes = S->pool_bytes;
+    return PP_SUCCESS;
+}
+
+extern "C" int pp_server_pool_stats(pp_server S, long long* created, long long* evicted)
+{
+    if (!S) return PP_INVALID_HANDLE;
+    std::lock_guard<std::mutex> g(S->mu);
+    if (created) *created = S->n_created;
+    if (evicted) *evicted = S->n_evicted;
     return PP_SUCCESS;
 }
 

@@ -13,11 +13,9 @@
 #include "../../include/pittpack_b200.h"
 #include "pp_common.cuh"
 #include "pp_kernels.h"
+#include "pp_tables.cuh"
 
 namespace {
-
-// the reference's constant (src/include/params.h: const double pi)
-const double REF_PI = 3.1415926535897932384;
 
 int kind_from_bc(char lo, char hi)
 {
@@ -157,26 +155,18 @@ int build_dir(pp_solver_s* h, DirTables& t, int n, int kind)
         }
     } else {
         cs.resize(n);
-        for (int k = 0; k < n; ++k) {
-            double theta = (REF_PI / 2. / n) * k;
-            cs[k] = make_double2(cos(theta), sin(theta));
-        }
+        for (int k = 0; k < n; ++k) cs[k] = pp_family_twiddle(n, k);
     }
-    // eigenvalue parts (setEigenVal src/pencilDcmp.cpp:3533-3576, getEigenVal 4393-4417)
-    double num = 0.0, den = 0.0, freq = REF_PI;
-    if (kind == PP_KIND_DST2) num = 1.0;
-    else if (kind == PP_KIND_FFT) freq = 2. * REF_PI;
-    else if (quarter) num = 0.5;
     std::vector<double> eig(n);
-    for (int k = 0; k < n; ++k) eig[k] = -2.0 + 2. * cos((k + num) * freq / (n + den));
+    for (int k = 0; k < n; ++k) eig[k] = pp_eigen_part(n, kind, k);
 
     cudaError_t e;
     if ((e = t.tw.alloc(sizeof(double2) * nf)) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
     if ((e = t.cs.alloc(sizeof(double2) * cs.size())) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
     if ((e = t.eig.alloc(sizeof(double) * n)) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
-    cudaMemcpy(t.tw.p, tw.data(), sizeof(double2) * nf, cudaMemcpyHostToDevice);
-    cudaMemcpy(t.cs.p, cs.data(), sizeof(double2) * cs.size(), cudaMemcpyHostToDevice);
-    if ((e = cudaMemcpy(t.eig.p, eig.data(), sizeof(double) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+    if ((e = cudaMemcpy(t.tw.p, tw.data(), sizeof(double2) * nf, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(t.cs.p, cs.data(), sizeof(double2) * cs.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(t.eig.p, eig.data(), sizeof(double) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUDA_ERROR);
     t.fft.tw = t.tw.as<double2>();
     // FP32 copies of the twiddles (rounded from the long-double / reference values)
@@ -185,8 +175,9 @@ int build_dir(pp_solver_s* h, DirTables& t, int n, int kind)
     for (size_t m = 0; m < cs.size(); ++m) csf[m] = make_float2((float)cs[m].x, (float)cs[m].y);
     if ((e = t.twf.alloc(sizeof(float2) * nf)) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
     if ((e = t.csf.alloc(sizeof(float2) * csf.size())) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
-    cudaMemcpy(t.twf.p, twf.data(), sizeof(float2) * nf, cudaMemcpyHostToDevice);
-    cudaMemcpy(t.csf.p, csf.data(), sizeof(float2) * csf.size(), cudaMemcpyHostToDevice);
+    if ((e = cudaMemcpy(t.twf.p, twf.data(), sizeof(float2) * nf, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(t.csf.p, csf.data(), sizeof(float2) * csf.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return set_cuda_error(h, e, PP_CUDA_ERROR);
     return PP_SUCCESS;
 }
 
@@ -215,19 +206,36 @@ int ref_tag_z(const char* bc)
     return t[2];
 }
 
-// exactValue (src/pencilDcmp.cpp:1837-1866)
-double exact_value(double omega, double x, int tg)
+// the manufactured-solution face parameters of a handle (modifyRhsDirichlet,
+// src/pencilDcmp.cpp:4623-4835): box corner, cell sizes, omega = {1, 2, 3} pi
+// and the reference's tags
+PPMmsFaces mms_faces(int nx, int ny, int nz, const char* bc, const double* box)
 {
-    if (fabs(omega) < 1.0e-6) return 1.0;
-    if (tg == 0 || tg == -1 || tg == -2) return sin(omega * x);
-    if (tg == 1) return cos(omega * x);
-    return 0.0;
+    PPMmsFaces p{};
+    p.nx = nx;
+    p.ny = ny;
+    p.nz = nz;
+    const double pi = 4. * atan(1.0);
+    p.Xa = box[0];
+    p.Ya = box[2];
+    p.Za = box[4];
+    p.c1 = -(box[0] - box[1]) / (nx);
+    p.c2 = -(box[2] - box[3]) / (ny);
+    p.c3 = -(box[4] - box[5]) / (nz);
+    p.omega[0] = 1 * pi;
+    p.omega[1] = 2 * pi;
+    p.omega[2] = 3 * pi;
+    p.t0 = ref_tag_xy(kind_from_bc(bc[0], bc[1]));
+    p.t1 = ref_tag_xy(kind_from_bc(bc[2], bc[3]));
+    p.t2 = ref_tag_z(bc);
+    return p;
 }
 
 // face corrections subtracted from the dz^2-scaled RHS: the caller's boundary
 // data where pp_set_face_values set some, else (option dirichlet_lift) the
 // manufactured-solution faces of modifyRhsDirichlet
 // (src/pencilDcmp.cpp:4623-4835), evaluated with the reference's expressions
+// (pp_mms_face_value)
 int build_lift(pp_solver_s* h)
 {
     for (auto& b : h->lift) b.free();
@@ -235,71 +243,34 @@ int build_lift(pp_solver_s* h)
     bool user = false;
     for (int f = 0; f < 6; ++f) user |= !h->uface[f].empty() && h->bc[f] != 'P';
     if (!h->opt.dirichlet_lift && !user) return PP_SUCCESS;
-    const int nx = h->nx, ny = h->ny, nz = h->nz;
-    const double pi = 4. * atan(1.0);
-    const double Xa = h->box[0], Ya = h->box[2], Za = h->box[4];
-    const double c1 = -(h->box[0] - h->box[1]) / (nx);
-    const double c2 = -(h->box[2] - h->box[3]) / (ny);
-    const double c3 = -(h->box[4] - h->box[5]) / (nz);
-    const double shift = 1.0;
-    const double omega[3] = {1 * pi, 2 * pi, 3 * pi};
-    const int t0 = ref_tag_xy(kind_from_bc(h->bc[0], h->bc[1]));
-    const int t1 = ref_tag_xy(kind_from_bc(h->bc[2], h->bc[3]));
-    const int t2 = ref_tag_z(h->bc);
+    const PPMmsFaces mp = mms_faces(h->nx, h->ny, h->nz, h->bc, h->box);
+    const double c1 = mp.c1, c2 = mp.c2, c3 = mp.c3;
     auto upload = [&](int face, const std::vector<double>& v) -> int {
         bool nonzero = false;
         for (double x : v) nonzero |= (x != 0.0);
         if (!nonzero) return PP_SUCCESS;  // nothing to subtract
         cudaError_t e = h->lift[face].alloc(sizeof(double) * v.size());
         if (e != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
-        cudaMemcpy(h->lift[face].p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice);
+        if ((e = cudaMemcpy(h->lift[face].p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return set_cuda_error(h, e, PP_CUDA_ERROR);
         return PP_SUCCESS;
     };
     int rc;
-    const bool manufactured = h->opt.dirichlet_lift != 0;
-    if (manufactured && (h->bc[4] == 'D' || h->bc[5] == 'D')) {
-        for (int face = 0; face < 2; ++face) {
-            if (h->bc[4 + face] != 'D' || !h->uface[4 + face].empty()) continue;
-            std::vector<double> v((size_t)nx * ny);
-            const double z = face == 0 ? Za : Za + (nz - 1) * c3 + c3;
-            for (int i = 0; i < nx; ++i) {
-                const double x = Xa + i * c1 + shift * c1 * .5;
-                for (int j = 0; j < ny; ++j) {
-                    const double y = Ya + j * c2 + shift * c2 * 0.5;
-                    v[i + (size_t)nx * j] =
-                        2. * exact_value(omega[0], x, t0) * exact_value(omega[1], y, t1) * exact_value(omega[2], z, t2);
-                }
-            }
-            if ((rc = upload(face, v)) != PP_SUCCESS) return rc;
+    if (h->opt.dirichlet_lift) {
+        // device slots: z faces 0, 1; x faces 2, 3; y faces 4, 5 (the caller's
+        // face numbers are xmin, xmax, ymin, ymax, zmin, zmax)
+        static const int face_of_slot[6] = {4, 5, 0, 1, 2, 3};
+        for (int slot = 0; slot < 6; ++slot) {
+            const int f = face_of_slot[slot];
+            if (h->bc[f] != 'D' || !h->uface[f].empty()) continue;
+            int na, nb;
+            pp_mms_face_dims(mp, slot, &na, &nb);
+            std::vector<double> v((size_t)na * nb);
+            for (int b = 0; b < nb; ++b)
+                for (int a = 0; a < na; ++a) v[a + (size_t)na * b] = pp_mms_face_value(mp, slot, a, b);
+            if ((rc = upload(slot, v)) != PP_SUCCESS) return rc;
         }
-    }
-    for (int face = 0; face < 2 && manufactured; ++face) {
-        if (h->bc[face] != 'D' || !h->uface[face].empty()) continue;
-        std::vector<double> v((size_t)ny * nz);
-        const double x = face == 0 ? Xa : Xa + ((nx - 1) + 1) * c1;
-        for (int k = 0; k < nz; ++k) {
-            const double z = Za + k * c3 + shift * c3 * .5;
-            for (int j = 0; j < ny; ++j) {
-                const double y = Ya + j * c2 + shift * c2 * 0.5;
-                v[j + (size_t)ny * k] =
-                    2. * exact_value(omega[0], x, t0) * exact_value(omega[1], y, t1) * exact_value(omega[2], z, t2);
-            }
-        }
-        if ((rc = upload(2 + face, v)) != PP_SUCCESS) return rc;
-    }
-    for (int face = 0; face < 2 && manufactured; ++face) {
-        if (h->bc[2 + face] != 'D' || !h->uface[2 + face].empty()) continue;
-        std::vector<double> v((size_t)nx * nz);
-        const double y = face == 0 ? Ya : Ya + ((ny - 1) + 1) * c2;
-        for (int k = 0; k < nz; ++k) {
-            const double z = Za + k * c3 + shift * c3 * .5;
-            for (int i = 0; i < nx; ++i) {
-                const double x = Xa + i * c1 + shift * c1 * 0.5;
-                v[i + (size_t)nx * k] =
-                    2. * exact_value(omega[0], x, t0) * exact_value(omega[1], y, t1) * exact_value(omega[2], z, t2);
-            }
-        }
-        if ((rc = upload(4 + face, v)) != PP_SUCCESS) return rc;
     }
     // the caller's data through the ghost-cell relations of the 7-point operator
     // scaled by dz^2: a face's neighbour term has weight w = (dz/dx)^2,
@@ -314,7 +285,6 @@ int build_lift(pp_solver_s* h)
             const double c = h->bc[f] == 'D' ? 2.0 * wgt[d] : wgt[d] * hh[d];
             std::vector<double> v(h->uface[f].size());
             for (size_t q = 0; q < v.size(); ++q) v[q] = c * h->uface[f][q];
-            // device slots: z faces 0, 1; x faces 2, 3; y faces 4, 5
             const int slot = d == 2 ? f - 4 : (d == 0 ? 2 + f : 4 + (f - 2));
             if ((rc = upload(slot, v)) != PP_SUCCESS) return rc;
         }
@@ -1249,7 +1219,7 @@ int pp_get_error_manufactured(pp_handle h, double* err)
     int rc = pp_get_solution(h, P.data());
     if (rc != PP_SUCCESS) return rc;
     // getError (src/pencilDcmp.cpp:2040-2208), INITANALYTIC = 1 branch
-    const double pi = REF_PI;
+    const double pi = PP_REF_PI;
     const double Xa = box[0], Ya = box[2], Za = box[4];
     const double c1 = -(box[0] - box[1]) / (nx);
     const double c2 = -(box[2] - box[3]) / (ny);
@@ -1273,8 +1243,8 @@ int pp_get_error_manufactured(pp_handle h, double* err)
                     val = P[2 * p] - (sin(omega[1] * z) * cos(omega[1] * (x + y)));
                     val1 = P[2 * p + 1] - (sin(omega[1] * z) * sin(omega[1] * (x + y)));
                 } else {
-                    val = P[2 * p] - exact_value(omega[0], x, t0) * exact_value(omega[1], y, t1) *
-                                         exact_value(omega[2], z, t2);
+                    val = P[2 * p] - pp_exact_value(omega[0], x, t0) * pp_exact_value(omega[1], y, t1) *
+                                         pp_exact_value(omega[2], z, t2);
                     val1 = 0.0;
                 }
                 if (pall) {
