@@ -90,9 +90,14 @@ def half_cols(n: int, bc: str, rhs_complex: bool = False, ny: int = 0) -> float:
 def kernel_bytes_per_point(bc: str, rhs_complex: bool = False, sweeps: int = -1, n: int = 512, ny: int = 0):
     """Algorithmic bytes per point of each stage.  sweeps < 0: the plain FP64
     solve; sweeps >= 0: the refined solve (FP32 spectra), summed over its
-    sweeps + 1 passes; the residual stage reads f and u (FP64) and writes r (FP32).
-    A periodic x spectrum of a real RHS is kept as half spectra (fraction h of
-    the columns), so everything between the x passes moves h times the bytes."""
+    sweeps + 1 passes.  Where x has a register-kernel length the forward x
+    pass forms the residual in its load: it reads f (FP64) every sweep and u
+    (FP64) from the second sweep on, and no residual array exists; otherwise
+    the residual stage reads f (and u) and writes r (FP32), which the forward
+    x pass reads.  The inverse x pass writes u (FP64) and, in the last sweep,
+    P (16 B); it reads u from the second sweep on.  A periodic x spectrum of a
+    real RHS is kept as half spectra (fraction h of the columns), so
+    everything between the x passes moves h times the bytes."""
     x_c = bc[0:2] == "PP"
     s_c = bc[2:4] == "PP"
     h = half_cols(n, bc, rhs_complex, ny)
@@ -103,11 +108,13 @@ def kernel_bytes_per_point(bc: str, rhs_complex: bool = False, sweeps: int = -1,
         return [r + X, X + S, 2 * S, 2 * S, S + 16, 0]
     X = (8 if x_c else 4) * h
     S = (8 if s_c else 4) * h
-    per = [4 + X, X + S, 2 * S, 2 * S, S + 8 + 8, 0]
-    tot = [p * (sweeps + 1) for p in per]
-    # residual: sweep 0 reads f and writes r; later sweeps also read u; the
-    # inverse-x update does not read u in sweep 0 and writes P (16 B) last
-    tot[5] = (8 + 4) + sweeps * (8 + 8 + 4)
+    k = sweeps + 1
+    tot = [0.0, (X + S) * k, 2 * S * k, 2 * S * k, (S + 8) * k + 8 * sweeps + 8, 0.0]
+    if n in LP2_LPC:
+        tot[0] = (8 + X) * k + 8 * sweeps
+    else:
+        tot[0] = (4 + X) * k
+        tot[5] = (8 + 4) + sweeps * (8 + 8 + 4)
     return tot
 
 
@@ -117,7 +124,10 @@ def launches_per_solve(bc: str, sweeps: int = -1) -> int:
         return 5
     zm = bc[0:2] in ("NN", "PP") and bc[2:4] in ("NN", "PP")
     singular = zm and bc[4] != "D" and bc[5] != "D"
-    return (sweeps + 1) * (6 + int(zm) + int(singular))
+    # five passes (plus the residual kernel for lengths outside the register
+    # kernel: not at the benchmark's 512); the zero-mode column: plane sums
+    # and its z solve, and the mean anchor when singular
+    return (sweeps + 1) * (5 + 2 * int(zm) + int(singular))
 
 
 def max_over_ranks(x: float, dist, device) -> float:

@@ -127,15 +127,21 @@ struct PPResidArgs {
     const double* f;   // real RHS, unscaled
     const double* u;   // current solution (real), or null for u = 0
     float* r;          // FP32 residual out
-    double* psum;      // per-plane sums of r times psum_scale (zero mode), or null
-    double psum_scale;
+    double* part;      // FP64 sums of r per (plane, xy tile): [nz][pp_resid_tiles], or null
     int nx, ny, nz;
     double dz, Cx, Cy;
     int bc[6];         // face codes: 0 Dirichlet, 1 Neumann, 2 periodic
     PPLift lift;
-    double* usum;      // FP64 sum of u over the grid, or null
+    double* upart;     // FP64 sums of u, same layout, or null
 };
+// xy tiles per plane of the residual kernel (the partial sums' row length)
+int pp_resid_tiles(int nx, int ny);
 cudaError_t pp_launch_resid(const PPResidArgs& a, cudaStream_t st);
+// The kx = ky = 0 column of a refined sweep from per-CTA partial sums
+// ([plane][tpp] each), added in a fixed order: zcol[k] = scale * sum_t
+// part[k tpp + t]; if upart is set, *usum = the sum of all of upart.
+cudaError_t pp_launch_zero_mode_sums(const double* part, const double* upart, int tpp, int nz, double scale,
+                                     double* zcol, double* usum, cudaStream_t st);
 // zero-mean solution (pp_mean.cu): the mean of the real parts of the n
 // complex-interleaved values of P is subtracted from them; scratch holds
 // pp_zero_mean_scratch_doubles() doubles

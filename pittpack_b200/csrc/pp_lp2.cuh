@@ -681,9 +681,10 @@ __global__ void __launch_bounds__(LPC * N / 8, lpm_min_blocks(LPC * N / 8)) lpm_
 {
     lp2_body<Real, N, LPC, FAM, INVERSE, STRIDED>(a);
 }
-// the periodic family's 512-point instances (complex lines, half spectra):
-// bounded to 48 registers, five CTAs of 256 threads per SM (measured faster;
-// the real families' instances spill under the same bound and are not)
+// the periodic family's 512-point FP64 instances (complex lines, half
+// spectra): bounded to 48 registers, five CTAs of 256 threads per SM
+// (measured faster; the real families' instances spill under the same bound
+// and are not)
 template <typename Real, int N, int LPC, int FAM, bool INVERSE, bool STRIDED>
 __global__ void __launch_bounds__(LPC * N / 8, 5) lp2b_kernel(PPLinePassArgs a)
 {
@@ -692,7 +693,7 @@ __global__ void __launch_bounds__(LPC * N / 8, 5) lp2b_kernel(PPLinePassArgs a)
 template <typename Real, int N, int LPC, int FAM, bool INVERSE, bool STRIDED>
 constexpr auto pass_kernel()
 {
-    if constexpr (N == 512 && (FAM == F_FFT || FAM == F_R2C || FAM == F_C2R))
+    if constexpr (N == 512 && (FAM == F_FFT || FAM == F_R2C || FAM == F_C2R) && std::is_same<Real, double>::value)
         return lp2b_kernel<Real, N, LPC, FAM, INVERSE, STRIDED>;
     else if constexpr ((N & (N - 1)) == 0) return lp2_kernel<Real, N, LPC, FAM, INVERSE, STRIDED>;
     else return lpm_kernel<Real, N, LPC, FAM, INVERSE, STRIDED>;

@@ -91,6 +91,7 @@ struct pp_solver_s {
     double* ext_out = nullptr;
     pp_tuning tune{0, 0, 0};  // launch-shape choices (0 = built-in default)
     DevBuf psum;   // refined solve: per-plane sums / zero-mode column (nz doubles)
+    DevBuf part;   // refined solve: per-CTA partial sums of r and of u (2 x nz x tiles)
     DevBuf zero1;  // one double 0.0 (eigen table of the zero-mode system)
     DevBuf mgstats;  // multigrid z solve: max cycles, unconverged systems (2 ints)
     DevBuf zmean;    // zero-mean option: partial sums and the mean
@@ -657,8 +658,12 @@ bool has_zero_mode(int kx, int ky)
 // M32 = FP32 transforms + FP64-arithmetic z solve on the FP32 spectrum with
 // the kx = ky = 0 column left out; that column (the only singular or nearly
 // singular one) is solved in FP64 from FP64 plane sums of r and added to u in
-// FP64.  The last sweep writes P.  Buffers: r (FP32) in the solution buffer,
-// FP32 spectra in the first halves of A and B, u (FP64) in the second half of B.
+// FP64.  The last sweep writes P.  The residual kernel (a z-marching 2.5-D
+// stencil) writes r (FP32) into the solution buffer; its per-(plane, tile)
+// FP64 partial sums of r are added in a fixed order for the zero-mode column
+// (the solve is bitwise reproducible).  Buffers: r (FP32) in the solution
+// buffer, FP32 spectra in the first halves of A and B, u (FP64) in the second
+// half of B.
 int launch_mixed(pp_solver_s* h)
 {
     const int nx = h->nx, ny = h->ny, nz = h->nz;
@@ -680,29 +685,38 @@ int launch_mixed(pp_solver_s* h)
     // singular: no Dirichlet end anywhere (the x/y families with a zero mode
     // are N-N or P-P)
     const bool singular = zm && h->bc[4] != 'D' && h->bc[5] != 'D';
+    const double* f = h->ext_rhs ? h->ext_rhs : h->rhs.as<double>();
+    double* u = reinterpret_cast<double*>(h->bufB.as<char>() + h->bufB.bytes / 2);
+    const int tpp = pp_resid_tiles(nx, ny);
     if (zm && !h->psum.p) {
         // zero-mode column (nz) + sum of u + target mean
         if ((e = h->psum.alloc(sizeof(double) * (nz + 2))) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
         if ((e = h->zero1.alloc(sizeof(double))) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
         if ((e = cudaMemset(h->zero1.p, 0, sizeof(double))) != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
     }
+    const size_t part_bytes = 2 * sizeof(double) * (size_t)nz * tpp;
+    if (zm && h->part.bytes < part_bytes && (e = h->part.alloc(part_bytes)) != cudaSuccess)
+        return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+    double* part = zm ? h->part.as<double>() : nullptr;
+    double* upart = zm ? part + (size_t)nz * tpp : nullptr;
+    const double psum_scale = (kx == PP_KIND_DCT2 ? 2.0 : 1.0) * (ky == PP_KIND_DCT2 ? 2.0 : 1.0);
     float* r32 = h->out.as<float>();
     float* A32 = h->bufA.as<float>();
     float* B32 = h->bufB.as<float>();
-    double* u = reinterpret_cast<double*>(h->bufB.as<char>() + h->bufB.bytes / 2);
+    int bcode[6];
+    for (int q = 0; q < 6; ++q) bcode[q] = h->bc[q] == 'P' ? 2 : (h->bc[q] == 'N' ? 1 : 0);
 
     PPResidArgs ra{};
-    ra.f = h->ext_rhs ? h->ext_rhs : h->rhs.as<double>();
+    ra.f = f;
     ra.r = r32;
-    ra.psum = zm ? h->psum.as<double>() : nullptr;
-    ra.psum_scale = (kx == PP_KIND_DCT2 ? 2.0 : 1.0) * (ky == PP_KIND_DCT2 ? 2.0 : 1.0);
+    ra.part = part;
     ra.nx = nx;
     ra.ny = ny;
     ra.nz = nz;
     ra.dz = dz;
     ra.Cx = (dz / dx) * (dz / dx);
     ra.Cy = (dz / dy) * (dz / dy);
-    for (int f = 0; f < 6; ++f) ra.bc[f] = h->bc[f] == 'P' ? 2 : (h->bc[f] == 'N' ? 1 : 0);
+    for (int q = 0; q < 6; ++q) ra.bc[q] = bcode[q];
     ra.lift = h->liftv;
 
     PPLinePassArgs ax{};
@@ -764,21 +778,12 @@ int launch_mixed(pp_solver_s* h)
     const int sweeps = h->opt.max_sweeps < 0 ? 0 : h->opt.max_sweeps;
     for (int sw = 0; sw <= sweeps; ++sw) {
         const bool last = sw == sweeps;
+        const bool want_usum = singular && sw > 0;
         t0 = stamp(h);
-        if (zm && (e = cudaMemsetAsync(h->psum.p, 0, sizeof(double) * (nz + 1), h->stream)) != cudaSuccess)
-            return set_cuda_error(h, e, PP_CUDA_ERROR);
         ra.u = sw == 0 ? nullptr : u;
-        ra.usum = (singular && sw > 0) ? h->psum.as<double>() + nz : nullptr;
+        ra.upart = want_usum ? upart : nullptr;
         if ((e = pp_launch_resid(ra, h->stream)) != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
-        if (zm && (e = pp_launch_zsolve(z0, false, h->stream)) != cudaSuccess)
-            return set_cuda_error(h, e, PP_THOMAS_FAIL);
-        if (singular &&
-            (e = pp_launch_zero_mode_anchor(h->psum.as<double>(), nz, h->psum.as<double>() + nz,
-                                            h->psum.as<double>() + nz + 1, 1.0 / (ra.psum_scale * (double)nx * ny),
-                                            (double)nx * ny * nz, sw == 0, h->stream)) != cudaSuccess)
-            return set_cuda_error(h, e, PP_CUDA_ERROR);
         stage_done(h, SLOT_RES, t0);
-
         PPLinePassArgs a1 = ax;
         a1.src = reinterpret_cast<const double*>(r32);
         a1.dst = reinterpret_cast<double*>(A32);
@@ -787,6 +792,20 @@ int launch_mixed(pp_solver_s* h)
         if ((e = line_pass(a1, h->tx, false, false, false, x_cplx, h->stream, true)) != cudaSuccess)
             return set_cuda_error(h, e, PP_CUFFT_FAIL_X);
         stage_done(h, SLOT_XF, t0);
+        if (zm) {
+            // the kx = ky = 0 column in FP64: plane sums, its z solve, the anchor
+            t0 = stamp(h);
+            double* ps = h->psum.as<double>();
+            if ((e = pp_launch_zero_mode_sums(part, want_usum ? upart : nullptr, tpp, nz, psum_scale, ps, ps + nz,
+                                              h->stream)) != cudaSuccess)
+                return set_cuda_error(h, e, PP_CUDA_ERROR);
+            if ((e = pp_launch_zsolve(z0, false, h->stream)) != cudaSuccess) return set_cuda_error(h, e, PP_THOMAS_FAIL);
+            if (singular &&
+                (e = pp_launch_zero_mode_anchor(ps, nz, ps + nz, ps + nz + 1, 1.0 / (psum_scale * (double)nx * ny),
+                                                (double)nx * ny * nz, sw == 0, h->stream)) != cudaSuccess)
+                return set_cuda_error(h, e, PP_CUDA_ERROR);
+            stage_done(h, SLOT_RES, t0);
+        }
         PPLinePassArgs a2 = ay;
         a2.src = reinterpret_cast<const double*>(A32);
         a2.dst = reinterpret_cast<double*>(B32);
@@ -812,7 +831,7 @@ int launch_mixed(pp_solver_s* h)
         a4.acc = u;
         a4.acc_read = sw > 0;
         a4.zplane = zm ? h->psum.as<double>() : nullptr;
-        a4.zscale = 1.0 / (ra.psum_scale * (double)nx * (double)ny);
+        a4.zscale = 1.0 / (psum_scale * (double)nx * (double)ny);
         a4.out_scale = 1. / ((double)(nx * ny));
         if (hc) set_half_in(a4, ncol, splane, nx, plane);
         t0 = stamp(h);
@@ -920,6 +939,7 @@ int pp_destroy(pp_handle h)
     for (auto& b : h->lift) b.free();
     timing_release(h);
     h->psum.free();
+    h->part.free();
     h->zero1.free();
     h->mgstats.free();
     h->zmean.free();
@@ -1328,7 +1348,7 @@ int pp_workspace_bytes(pp_handle h, size_t* bytes)
     for (auto& l : h->lift) b += l.bytes;
     for (const DirTables* t : {&h->tx, &h->ty})
         b += t->tw.bytes + t->cs.bytes + t->eig.bytes + t->twf.bytes + t->csf.bytes;
-    b += h->psum.bytes + h->zero1.bytes + h->mgstats.bytes + h->zmean.bytes;
+    b += h->psum.bytes + h->part.bytes + h->zero1.bytes + h->mgstats.bytes + h->zmean.bytes;
     *bytes = b;
     return PP_SUCCESS;
 }

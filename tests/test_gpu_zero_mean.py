@@ -2,11 +2,10 @@
 src/pencilDcmp.cpp:5649-5683): after the solve the mean of the solution's
 real part over the grid is subtracted from it.  Checked against the plain
 solve minus its own mean, for a pure-Neumann (singular, zero-mean RHS) and a
-Dirichlet problem, in FP64 and in the refined mode.  The mean is summed in
-a fixed order, so repeated FP64 solves give the same bits; the refined mode's
-plane sums are accumulated with one atomic per CTA, so its repeats agree to
-round-off.  The golden files under tests/golden/zero_mean/ pin it to the
-reference's own ZERO_MEAN build."""
+Dirichlet problem, in FP64 and in the refined mode.  The mean, and the
+refined mode's plane sums, are summed in a fixed order, so repeated solves
+give the same bits in both precisions.  The golden files under
+tests/golden/zero_mean/ pin it to the reference's own ZERO_MEAN build."""
 import glob
 import os
 
@@ -64,10 +63,7 @@ def test_zero_mean_subtracts_the_solution_mean(bc, precision):
     assert abs(P1.real.mean()) <= 1e-13 * scale
     assert np.abs(P1.real - ref).max() <= 1e-12 * scale
     assert np.array_equal(P1.imag, P0.imag)
-    if precision == 0:
-        assert np.array_equal(P1, P2)
-    else:
-        assert np.abs(P1 - P2).max() <= 1e-14 * scale
+    assert np.array_equal(P1, P2)
 
 
 def test_zero_mean_option_is_validated():
