@@ -18,10 +18,18 @@ Metric: Mpoints/s = grid points solved / time.
 `value` times the solves with the RHS already resident in HBM (CUDA events on
 the solver stream, max over ranks); `e2e` times the public API end to end:
 per grid, page-locked host RHS -> pp_assign_rhs_async (H2D) -> pp_solve ->
-pp_get_solution_async (D2H of the complex-interleaved solution), the four
-grids on four streams so that their copies overlap, wall clock until every
-stream has finished.  Inputs (1 GiB per grid) are larger than the 126 MB L2,
-so no flush is needed between solves.
+pp_get_solution_real_async (D2H of the solution's real part: the RHS is real,
+so the imaginary part is zero), the four grids on four streams so that their
+copies overlap, wall clock until every stream has finished; the same with
+the complex-interleaved chunkedArray P (pp_get_solution_async, twice the
+bytes down) is reported beside it.  Inputs (1 GiB per grid) are larger than
+the 126 MB L2, so no flush is needed between solves.
+
+While the GPU is timed, two spawned CPU processes solve the first family's
+RHS (NNNNDD when the four are run): the reference's own CPU path (its time is
+`cpu_baseline`, one core, on the benchmark's 512^3 grid; its solution checks
+the timed FP64 solve) and the oracle's exact-zero-mode solve (it checks the
+refined solve); the relative L2 errors are in `parity_512`.
 
 Two more workloads are reported beside the headline (skip with --no-batch /
 --no-serve): `batch`, 96 uneven grids (seed 7) solved by one CUDA-graph
@@ -32,9 +40,10 @@ Multi-GPU: the solve does not shard (one grid per GPU); N ranks run N
 independent replicas of the workload and `value` counts the points of all.
 
 `--impl reference` times the reference's own CPU path (PencilDcmp::pittPack
-of the PittPack sources, built single-rank by oracle/Makefile) on one host
-core on a bounded sample: one 128^3 grid per family it supports (PP, NN, DD;
-it has no N-D family) per step.
+of the PittPack sources, built single-rank by oracle/Makefile) on the
+benchmark's 512^3 grid: as many concurrent single-rank replicas as the host's
+cores and memory allow, the families it supports (PP, NN, DD; it has no N-D
+family) in turn, one solve each.
 """
 from __future__ import annotations
 
@@ -429,104 +438,123 @@ def run_serve_leg(args):
 
 
 REF_FAMILIES = ["PPPPDD", "NNNNDD", "DDDDDD"]
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libppref.so")
 
 
-def _ref_solver(n: int):
-    """One n^3 solve of the reference's CPU path (its own sources built by
-    oracle/Makefile), or of the oracle restatement when that build is absent.
-    Returns (solve(bc), kind)."""
+def _quiet_call(fn):
+    """Run fn with the process's stdout silenced (the reference prints its set-up)."""
+    fd = os.dup(1)
+    nul = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(nul, 1)
+    try:
+        return fn()
+    finally:
+        os.dup2(fd, 1)
+        os.close(fd)
+        os.close(nul)
+
+
+def reference_solve(n: int, bc: str, f, out=None):
+    """One n^3 solve of the reference's CPU path: PencilDcmp::pittPack of its
+    own sources built single-rank by oracle/Makefile (the shim's FP64 FFT in
+    place of FFTW); returns (P as complex128 (n, n, n), seconds)."""
     import numpy as np
 
-    lib = os.path.join(ROOT, "oracle", "_ref", "libppref.so")
-    rng = np.random.default_rng(11)
-    f = rng.uniform(-1, 1, n ** 3)
-    out = np.zeros(2 * n ** 3)
-    box = np.array([0, 1, 0, 1, 0, 1.0])
+    os.environ["PP_SHIM_FFT"] = "fast"
+    L = ctypes.CDLL(REF_LIB)
     dp = ctypes.POINTER(ctypes.c_double)
-    if os.path.exists(lib):
-        os.environ["PP_SHIM_FFT"] = "fast"
-        L = ctypes.CDLL(lib)
-        L.ppref_solve.argtypes = [ctypes.c_int] * 3 + [ctypes.c_char_p, dp, dp, dp, dp, dp]
-        kind = "reference"
-
-        def one(bc):
-            sec = ctypes.c_double()
-            # silence the reference's console output
-            fd = os.dup(1)
-            nul = os.open(os.devnull, os.O_WRONLY)
-            os.dup2(nul, 1)
-            try:
-                L.ppref_solve(n, n, n, bc.encode(), box.ctypes.data_as(dp), f.ctypes.data_as(dp), None,
-                              out.ctypes.data_as(dp), ctypes.byref(sec))
-            finally:
-                os.dup2(fd, 1)
-                os.close(fd)
-                os.close(nul)
-    else:
-        from oracle import oracle as O
-
-        kind = "port"
-
-        def one(bc):
-            O.solve(O.problem(n, n, n, bc), f.reshape(n, n, n))
-    return one, kind
-
-
-def _ref_sample_text(steps: int, n: int, kind: str) -> str:
-    return (f"{steps} step(s) x {len(REF_FAMILIES)} families (PPPPDD, NNNNDD, DDDDDD) of a {n}^3 grid, "
-            f"{'shim FFT in place of FFTW (absent)' if kind == 'reference' else 'oracle restatement'}")
-
-
-def cpu_reference_sample(steps: int, warmup: int, n: int = 128):
-    """The reference's CPU path on one core: one n^3 solve per family it
-    supports per step.  Returns (Mpoints/s, kind, cores, sample text)."""
-    one, kind = _ref_solver(n)
-    for _ in range(warmup):
-        one(REF_FAMILIES[0])
+    L.ppref_solve.argtypes = [ctypes.c_int] * 3 + [ctypes.c_char_p, dp, dp, dp, dp, dp]
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    if out is None:
+        out = np.zeros(2 * f.size)
+    box = np.array([0, 1, 0, 1, 0, 1.0])
+    sec = ctypes.c_double()
     t0 = time.perf_counter()
-    for _ in range(steps):
-        for bc in REF_FAMILIES:
-            one(bc)
-    dt = time.perf_counter() - t0
-    pts = steps * len(REF_FAMILIES) * n ** 3
-    return pts / dt / 1e6, kind, 1, _ref_sample_text(steps, n, kind)
+    _quiet_call(lambda: L.ppref_solve(n, n, n, bc.encode(), box.ctypes.data_as(dp), f.ctypes.data_as(dp), None,
+                                      out.ctypes.data_as(dp), ctypes.byref(sec)))
+    return out.view(np.complex128).reshape(n, n, n), time.perf_counter() - t0
 
 
-def _ref_replica(steps: int, warmup: int, n: int, barrier, queue) -> None:
-    """One single-rank replica of the reference's CPU path, in a process of
-    its own: warm up, wait for the others, time the steps."""
+def _cpu_job(kind: str, n: int, bc: str, f_path: str, out_path: str):
+    """Worker of the bench's CPU legs (a spawned process): the reference's own
+    solve ("reference", timed) or the oracle's exact-zero-mode solve
+    ("oracle") of the RHS stored at f_path; the solution goes to out_path.
+    Returns (kind, seconds, status)."""
+    import numpy as np
+
     try:
-        one, kind = _ref_solver(n)
-        for _ in range(warmup):
-            one(REF_FAMILIES[0])
+        f = np.load(f_path, mmap_mode="r")
+        if kind == "reference":
+            P, sec = reference_solve(n, bc, f)
+        else:
+            from oracle import oracle as O
+
+            t0 = time.perf_counter()
+            P = O.solve(O.problem(n, n, n, bc, compat_zero_mode=0), np.ascontiguousarray(f))
+            sec = time.perf_counter() - t0
+        np.save(out_path, P)
+        return kind, sec, "ok"
+    except Exception as e:  # reported in the JSON line
+        return kind, 0.0, f"error: {e}"
+
+
+def rel_l2_files(a, b_path: str, chunk: int = 1 << 24) -> float:
+    """Relative L2 of a against the array stored at b_path, in chunks."""
+    import numpy as np
+
+    b = np.load(b_path, mmap_mode="r").reshape(-1)
+    a = np.asarray(a).reshape(-1)
+    num = den = 0.0
+    for s0 in range(0, a.size, chunk):
+        d = a[s0:s0 + chunk] - b[s0:s0 + chunk]
+        num += float(np.vdot(d, d).real)
+        den += float(np.vdot(b[s0:s0 + chunk], b[s0:s0 + chunk]).real)
+    return (num / den) ** 0.5 if den > 0 else 0.0
+
+
+def _ref_replica(n: int, bc: str, barrier, queue) -> None:
+    """One single-rank replica of the reference's CPU path on the benchmark's
+    grid, in a process of its own: build the RHS, wait for the others, solve."""
+    try:
+        import numpy as np
+
+        f = np.random.default_rng(11).uniform(-1, 1, (n, n, n))
+        out = np.zeros(2 * n ** 3)
         barrier.wait(timeout=600)
-        t0 = time.perf_counter()
-        for _ in range(steps):
-            for bc in REF_FAMILIES:
-                one(bc)
-        queue.put((steps * len(REF_FAMILIES) * n ** 3, time.perf_counter() - t0, kind))
+        _, sec = reference_solve(n, bc, f, out)
+        queue.put((n ** 3, sec, "reference"))
     except Exception as e:  # reported to the parent, which fails the run
         barrier.abort()
         queue.put((0, 0.0, f"error: {e}"))
 
 
-def cpu_reference_parallel(steps: int, warmup: int, n: int = 128, workers: int = 0):
-    """The reference's CPU path on all host cores it can use.  The reference
-    runs one MPI rank per core on pencils of one grid; its single-rank build
-    here runs one independent replica per core instead (same arithmetic, no
-    exchanges), all timed together: Mpoints/s = all replicas' points / the
-    slowest replica's time.  Returns (Mpoints/s, kind, cores, sample text)."""
+def cpu_reference_parallel(n: int = N_GRID, workers: int = 0):
+    """The reference's CPU path on the host's cores, on the benchmark's own
+    grid.  The reference runs one MPI rank per core on pencils of one grid; its
+    single-rank build runs one independent grid per core instead (same
+    arithmetic, no exchanges): the replicas take the families PP, NN, DD in
+    turn, as many as the cores and the memory allow (about 11 GB each at
+    512^3), all timed together: Mpoints/s = all replicas' points / the slowest
+    replica's time.  Returns (Mpoints/s, cores, sample text)."""
     import multiprocessing as mp
 
     if workers <= 0:
-        workers = max(1, min(64, len(os.sched_getaffinity(0))))
+        cores = max(1, min(64, len(os.sched_getaffinity(0))))
+        try:
+            import psutil
+
+            by_mem = int(psutil.virtual_memory().available * 0.7 // (11e9 * (n / 512) ** 3))
+        except Exception:
+            by_mem = 4
+        workers = max(1, min(cores, by_mem))
     ctx = mp.get_context("spawn")
     barrier, queue = ctx.Barrier(workers), ctx.Queue()
-    procs = [ctx.Process(target=_ref_replica, args=(steps, warmup, n, barrier, queue)) for _ in range(workers)]
+    fams = [REF_FAMILIES[i % len(REF_FAMILIES)] for i in range(workers)]
+    procs = [ctx.Process(target=_ref_replica, args=(n, bc, barrier, queue)) for bc in fams]
     for p in procs:
         p.start()
     try:
-        res = [queue.get(timeout=1800) for _ in range(workers)]
+        res = [queue.get(timeout=3600) for _ in range(workers)]
     finally:
         for p in procs:
             p.join(timeout=60)
@@ -535,23 +563,27 @@ def cpu_reference_parallel(steps: int, warmup: int, n: int = 128, workers: int =
         raise RuntimeError(f"reference replica failed: {bad[0]}")
     pts = sum(r[0] for r in res)
     dt = max(r[1] for r in res)
-    kind = res[0][2]
-    sample = f"{workers} concurrent single-rank replicas (one per core), each " + _ref_sample_text(steps, n, kind)
-    return pts / dt / 1e6, kind, workers, sample
+    sample = (f"{workers} concurrent single-rank replicas (one per core, memory-bound count), each one solve "
+              f"of a {n}^3 grid, families {', '.join(sorted(set(fams)))} in turn; shim FFT in place of FFTW (absent)")
+    return pts / dt / 1e6, workers, sample
 
 
 def run_reference(args):
     rank, _, world = env_rank()
     if rank != 0:
         return 0
-    v, kind, cores, sample = cpu_reference_parallel(max(1, args.steps), max(0, min(args.warmup, 1)))
+    if not os.path.exists(REF_LIB):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libppref.so not built "
+                                                              "(make -C oracle PITTPACK_SRC=<PittPack tree>)"}))
+        return 0
+    v, cores, sample = cpu_reference_parallel(args.n)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "reference CPU path, bounded sample (see cpu_baseline.sample)", "grid": 128,
-                   "families": ["PPPPDD", "NNNNDD", "DDDDDD"]},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (i.i.d. U(-1,1) RHS, seed 11)",
+        "config": {"workload": f"reference CPU path, {args.n}^3 grid, one solve per replica (see cpu_baseline.sample)",
+                   "grid": [args.n] * 3, "families": REF_FAMILIES},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -592,6 +624,22 @@ def run_ours(args):
         solvers.append(M)
         rhs_dev.append(f)
     torch.cuda.synchronize()
+
+    # CPU legs, started now so that they run while the GPU is timed: the
+    # reference's own solve of the first family the reference has (its time is
+    # the CPU baseline on the benchmark's grid; its solution checks the FP64
+    # solve timed here) and the oracle's exact-zero-mode solve of the same RHS
+    # (checks the refined solve)
+    cpu_pool = cpu_jobs = None
+    cpu_fam = next((bc for bc in FAMILIES if bc in REF_FAMILIES), None)
+    tmp = os.path.join("/tmp", f"pp_bench_{os.getpid()}")
+    if rank == 0 and world == 1 and not args.no_cpu and cpu_fam and os.path.exists(REF_LIB) and nx == ny == nz:
+        import multiprocessing as mp
+
+        np.save(tmp + "_f.npy", rhs_dev[FAMILIES.index(cpu_fam)].cpu().numpy())
+        cpu_pool = mp.get_context("spawn").Pool(2)
+        cpu_jobs = [cpu_pool.apply_async(_cpu_job, (k, nx, cpu_fam, tmp + "_f.npy", f"{tmp}_{k}.npy"))
+                    for k in ("reference", "oracle")]
 
     peak, peak_kind = hbm_peak()
     modes = {"fp64": dict(precision=0, compat_zero_mode=1, max_sweeps=0),
@@ -694,6 +742,43 @@ def run_ours(args):
     results["mixed"]["rel_err_vs_fp64"] = max(errs)
     results["mixed"]["rel_err_per_family"] = dict(zip(FAMILIES, errs))
     results["mixed"]["sweeps"] = args.sweeps
+
+    # the CPU legs: the timed FP64 solve (the reference's zero-mode semantics)
+    # against the reference's own solve, the refined solve against the oracle
+    cpu = parity = None
+    if cpu_jobs is not None:
+        M = solvers[FAMILIES.index(cpu_fam)]
+        host = np.empty(2 * npts, dtype=np.float64)
+        outcome = {}
+        for job in cpu_jobs:
+            kind, sec, status = job.get(timeout=3600)
+            outcome[kind] = (sec, status)
+        parity = {"family": cpu_fam, "grid": [nx, ny, nz]}
+        for name, kind in (("fp64", "reference"), ("mixed", "oracle")):
+            sec, status = outcome[kind]
+            if status != "ok":
+                parity[name] = status
+                continue
+            M.setOptions(**modes[name])
+            M.pittPack()
+            M.solutionToDevice(ref_buf.data_ptr())
+            torch.cuda.synchronize()
+            host[:] = ref_buf.cpu().numpy()
+            err = rel_l2_files(host.view(np.complex128), f"{tmp}_{kind}.npy")
+            parity[name] = {"against": "reference's own pittPack()" if kind == "reference"
+                            else "oracle, exact zero mode", "rel_l2": err}
+        if outcome["reference"][1] == "ok":
+            cpu = {"value": npts / outcome["reference"][0] / 1e6, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"one solve of the benchmark's {nx}^3 {cpu_fam} grid (the timed RHS) by the reference's "
+                             f"own CPU path on one host core, shim FFT in place of FFTW (absent)"}
+        cpu_pool.close()
+        cpu_pool.join()
+        for suffix in ("_f.npy", "_reference.npy", "_oracle.npy"):
+            try:
+                os.remove(tmp + suffix)
+            except OSError:
+                pass
+        del host
     best = "mixed" if (results["mixed"]["rel_err_vs_fp64"] <= 1e-10
                        and results["mixed"]["value"] > results["fp64"]["value"]) else "fp64"
     value = results[best]["value"]
@@ -711,34 +796,43 @@ def run_ours(args):
     # one stream and one page-locked output per grid: the four solves are
     # issued with the asynchronous public calls, so one grid's upload overlaps
     # another's download and compute
-    h_out = [pinned_empty((nz, ny, nx), np.complex128) for _ in solvers]
+    # the solution's real part (a real RHS: the imaginary part is zero), and
+    # the reference's complex-interleaved P beside it
+    h_out = [pinned_empty((nz, ny, nx), np.float64) for _ in solvers]
+    h_outc = [pinned_empty((nz, ny, nx), np.complex128) for _ in solvers]
     e2e_streams = [torch.cuda.Stream() for _ in solvers]
     for M, s in zip(solvers, e2e_streams):
         M.setStream(s.cuda_stream)
     e2e_steps = max(1, min(args.steps, 3))
 
-    def e2e_step():
-        for M, a, o in zip(solvers, h_rhs, h_out):
+    def e2e_step(real):
+        for M, a, o, oc in zip(solvers, h_rhs, h_out, h_outc):
             M.assignRhsAsync(a)
             M.pittPack()
-            M.getSolutionAsync(o)
+            if real:
+                M.getSolutionRealAsync(o)
+            else:
+                M.getSolutionAsync(oc)
         for M in solvers:
             M.synchronize()
 
-    e2e_step()  # warm-up of the copy path
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    w0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        e2e_step()
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - w0, dist, "cuda")
-    e2e_val = replica_throughput(world, e2e_steps * len(FAMILIES) * npts, e2e_s)
+    e2e = {}
+    for real in (True, False):
+        e2e_step(real)  # warm-up of the copy path
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step(real)
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - w0, dist, "cuda")
+        e2e["real" if real else "complex"] = replica_throughput(world, e2e_steps * len(FAMILIES) * npts, e2e_s)
+    e2e_val = e2e["real"]
 
     for M in solvers:
         M.close()
-    del h_rhs, h_out, ref_buf, mix_buf
+    del h_rhs, h_out, h_outc, ref_buf, mix_buf
     torch.cuda.empty_cache()
     batch = serve = None
     if world == 1 and not args.no_batch:
@@ -746,10 +840,6 @@ def run_ours(args):
     if world == 1 and not args.no_serve:
         serve = run_serve_leg(args)
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        v, kind, cores, sample = cpu_reference_sample(1, 0)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
     if rank == 0:
         line = {
@@ -769,7 +859,11 @@ def run_ours(args):
             "kernels": results[best]["kernels"],
             "modes": results,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": len(FAMILIES) * npts * 8,
-                    "d2h_bytes_per_step": len(FAMILIES) * npts * 16, "steps": e2e_steps, "mode": best},
+                    "d2h_bytes_per_step": len(FAMILIES) * npts * 8, "steps": e2e_steps, "mode": best,
+                    "output": "the solution's real part (pp_get_solution_real_async)",
+                    "complex_P": {"value": e2e["complex"], "d2h_bytes_per_step": len(FAMILIES) * npts * 16,
+                                  "output": "complex-interleaved chunkedArray P (pp_get_solution_async)"}},
+            "parity_512": parity,
             "gpu_launches": results[best]["gpu_launches"],
             "clocks": clk,
             "cpu_baseline": cpu,

@@ -83,6 +83,8 @@ class PoissonB200 {
     void pittPack() { check(pp_solve(h_), "pittPack"); }
     // P in the chunkedArray layout: 2*nx*ny*nz doubles
     void getSolution(double* P) { check(pp_get_solution(h_, P), "getSolution"); }
+    // the real part alone (nx*ny*nz doubles): half the bytes, for a real RHS
+    void getSolutionReal(double* u) { check(pp_get_solution_real(h_, u), "getSolutionReal"); }
     double getError()
     {
         double e = 0.0;

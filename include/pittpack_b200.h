@@ -161,6 +161,14 @@ int pp_solution_device_ptr(pp_handle h, const double** d_P);
 /* the solution to host memory on the handle's stream without waiting (P
  * page-locked for a truly asynchronous copy); no counterpart in the reference */
 int pp_get_solution_async(pp_handle h, double* P);
+/* the real part of the solution alone, u[i] = P[2 i] (nx*ny*nz doubles, x
+ * fastest): half the bytes of P over PCIe, for callers with a real RHS, whose
+ * solution's imaginary part is zero (a complex periodic RHS needs the full P).
+ * Packed on the device on the handle's stream, then copied; the _async form
+ * returns without waiting (u page-locked for a truly asynchronous copy).  No
+ * counterpart in the reference, which leaves the complex P in host memory. */
+int pp_get_solution_real(pp_handle h, double* u);
+int pp_get_solution_real_async(pp_handle h, double* u);
 
 /* getError (src/pencilDcmp.cpp:2040-2208): RMS error of the solution against
  * the reference's manufactured solution; does not modify the solution */

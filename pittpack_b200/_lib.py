@@ -90,6 +90,8 @@ def load():
         "pp_workspace_bytes": ([H, ctypes.POINTER(ctypes.c_size_t)], i),
         "pp_assign_rhs_async": ([H, ctypes.c_void_p], i),
         "pp_get_solution_async": ([H, ctypes.c_void_p], i),
+        "pp_get_solution_real": ([H, ctypes.c_void_p], i),
+        "pp_get_solution_real_async": ([H, ctypes.c_void_p], i),
         "pp_bind_device_buffers": ([H, ctypes.c_void_p, i, ctypes.c_void_p], i),
         "pp_set_tuning": ([H, ctypes.POINTER(Tuning)], i),
         "pp_get_tuning": ([H, ctypes.POINTER(Tuning)], i),

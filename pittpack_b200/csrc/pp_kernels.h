@@ -147,6 +147,8 @@ cudaError_t pp_launch_zero_mode_sums(const double* part, const double* upart, in
 // pp_zero_mean_scratch_doubles() doubles
 size_t pp_zero_mean_scratch_doubles();
 cudaError_t pp_launch_zero_mean(double* P, long n, double* scratch, cudaStream_t st);
+// u[i] = P[2 i] for the n complex-interleaved values of P (P 16-byte aligned)
+cudaError_t pp_launch_real_part(const double* P, double* u, long n, cudaStream_t st);
 // Singular problems: keep the null-space constant of the refined solution at
 // the value implied by the pinned FP64 zero-mode solve of b (see pp_mixed.cu).
 cudaError_t pp_launch_zero_mode_anchor(double* zcol, int nz, const double* usum, double* mstar, double zscale,

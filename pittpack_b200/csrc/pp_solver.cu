@@ -1199,6 +1199,28 @@ int pp_get_solution_async(pp_handle h, double* P)
     return e == cudaSuccess ? PP_SUCCESS : set_cuda_error(h, e, PP_CUDA_ERROR);
 }
 
+// the real part of the solution packed into the (free after the solve)
+// workspace A, copied to the host; the caller's next solve on this handle's
+// stream starts after the copy
+static int get_real(pp_handle h, double* u, bool wait)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!u) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    cudaSetDevice(h->device);
+    const size_t n = (size_t)h->nx * h->ny * h->nz;
+    const double* src = h->ext_out ? h->ext_out : h->out.as<double>();
+    if (reinterpret_cast<uintptr_t>(src) % 16) return PP_INPUT_ARGS;
+    double* pack = h->bufA.as<double>();
+    cudaError_t e = pp_launch_real_part(src, pack, (long)n, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(u, pack, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && wait) e = cudaStreamSynchronize(h->stream);
+    return e == cudaSuccess ? PP_SUCCESS : set_cuda_error(h, e, PP_CUDA_ERROR);
+}
+
+int pp_get_solution_real(pp_handle h, double* u) { return get_real(h, u, true); }
+int pp_get_solution_real_async(pp_handle h, double* u) { return get_real(h, u, false); }
+
 int pp_get_solution_device(pp_handle h, double* d_P)
 {
     if (!h) return PP_INVALID_HANDLE;

@@ -221,6 +221,26 @@ class PoissonGPU:
             raise PittPackError(_lib.PP_INPUT_ARGS, "getSolutionAsync needs a contiguous complex128 array of nx*ny*nz")
         check(self._L.pp_get_solution_async(self._h, out.ctypes.data), "pp_get_solution_async")
 
+    def getSolutionReal(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The real part of the solution alone (float64, shape (nz, ny, nx)):
+        half the bytes of getSolution, for a real RHS (whose solution has a
+        zero imaginary part)."""
+        n = self.nx * self.ny * self.nz
+        if out is None:
+            out = np.empty((self.nz, self.ny, self.nx), dtype=np.float64)
+        if not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous and out.size == n):
+            raise PittPackError(_lib.PP_INPUT_ARGS, "getSolutionReal needs a contiguous float64 array of nx*ny*nz")
+        check(self._L.pp_get_solution_real(self._h, out.ctypes.data), "pp_get_solution_real")
+        return out
+
+    def getSolutionRealAsync(self, out: np.ndarray) -> None:
+        """getSolutionReal on the handle's stream without waiting (out
+        page-locked for an asynchronous copy); synchronize() before reading it."""
+        if not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+                and out.size == self.nx * self.ny * self.nz):
+            raise PittPackError(_lib.PP_INPUT_ARGS, "getSolutionRealAsync needs a contiguous float64 array of nx*ny*nz")
+        check(self._L.pp_get_solution_real_async(self._h, out.ctypes.data), "pp_get_solution_real_async")
+
     def setTuning(self, zsolve_lanes: int = 0, line_tile: int = 0, zsolve_tile: int = 0) -> None:
         t = _lib.Tuning(int(zsolve_lanes), int(line_tile), int(zsolve_tile))
         check(self._L.pp_set_tuning(self._h, ctypes.byref(t)), "pp_set_tuning")
