@@ -360,8 +360,11 @@ def run_batch_leg(args, torch, stream):
 def run_serve_leg(args):
     """Poisson arrivals of single solves (seed 11) at each rate; host RHS in
     page-locked memory -> server (H2D, solve, D2H on one of 8 streams) -> host
-    solution.  Latency is counted from the scheduled arrival, so time a request
-    waits on the client side (at most 10 outstanding) is included."""
+    solution, either the complex chunkedArray P or its real part alone (half
+    the copy).  Latency is counted from the scheduled arrival, so time a
+    request waits on the client side (at most 10 outstanding) is included.
+    Handle creations and evictions during each rate's stream are counted (a
+    creation allocates device memory, an eviction frees it; both stall)."""
     import numpy as np
 
     from pittpack_b200.batch import Server
@@ -373,67 +376,77 @@ def run_serve_leg(args):
     rng = np.random.default_rng(11)
     rhs = pinned_empty((nmax ** 3,), np.float64)
     rhs[...] = rng.standard_normal(nmax ** 3)
-    ring = [pinned_empty((nmax ** 3,), np.complex128) for _ in range(10)]
+    rings = {"complex": [pinned_empty((nmax ** 3,), np.complex128) for _ in range(10)],
+             "real": [pinned_empty((nmax ** 3,), np.float64) for _ in range(10)]}
     pts = sum(n ** 3 for n, _ in reqs)
     out = {}
     for name, prec in (("fp64", 0), ("mixed", 1)):
-        # a budget that holds every warmed shape: no handle is created or
-        # evicted (cudaFree waits for the device) while requests arrive
-        S = Server(streams=8, hbm_fraction=0.85)
-        # plans, twiddles and workspaces resident before the stream starts
-        seen = set()
-        for n, bc in reqs:
-            if (n, bc) not in seen:
-                seen.add((n, bc))
-                st, _, _ = S.wait(S.submit(n, n, n, bc, rhs[:n ** 3], ring[0][:n ** 3], precision=prec,
-                                           sweeps=args.sweeps))
-                if st != 0:
-                    raise RuntimeError(f"warm-up request {n}^3 {bc} failed with status {st}")
-        # and the whole stream once back to back (10 outstanding), so that the
-        # pool also holds the second handles of shapes that overlap in flight
-        wt = []
-        for i, (n, bc) in enumerate(reqs):
-            if i >= len(ring):
-                S.wait(wt[i - len(ring)])
-            wt.append(S.submit(n, n, n, bc, rhs[:n ** 3], ring[i % len(ring)][:n ** 3], precision=prec,
-                               sweeps=args.sweeps))
-        for t in wt[max(0, count - len(ring)):]:
-            S.wait(t)
-        per_rate = []
-        for rate in SERVE_RATES:
-            arr = np.cumsum(np.random.default_rng(11 + rate).exponential(1.0 / rate, count))
-            tickets, t_sub = [], []
-            lat, ends, used = [0.0] * count, [0.0] * count, [0] * count
-            t0 = time.perf_counter()
-
-            def collect(i):
-                st, ms, pu = S.wait(tickets[i])
-                if st != 0:
-                    raise RuntimeError(f"request {i} failed with status {st}")
-                lat[i] = (t_sub[i] - (t0 + arr[i])) * 1e3 + ms
-                ends[i] = t_sub[i] + ms / 1e3
-                used[i] = pu
-
+        out[name] = {}
+        for output in ("complex", "real"):
+            ring = rings[output]
+            # a budget that holds every warmed shape: no handle is created or
+            # evicted (cudaFree waits for the device) while requests arrive
+            S = Server(streams=8, hbm_fraction=0.85)
+            # plans, twiddles and workspaces resident before the stream starts
+            seen = set()
+            for n, bc in reqs:
+                if (n, bc) not in seen:
+                    seen.add((n, bc))
+                    st, _, _ = S.wait(S.submit(n, n, n, bc, rhs[:n ** 3], ring[0][:n ** 3], precision=prec,
+                                               sweeps=args.sweeps))
+                    if st != 0:
+                        raise RuntimeError(f"warm-up request {n}^3 {bc} failed with status {st}")
+            # and the whole stream once back to back (10 outstanding), so that the
+            # pool also holds the second handles of shapes that overlap in flight
+            wt = []
             for i, (n, bc) in enumerate(reqs):
-                while time.perf_counter() < t0 + arr[i]:
-                    pass
                 if i >= len(ring):
-                    collect(i - len(ring))
-                t_sub.append(time.perf_counter())
-                tickets.append(S.submit(n, n, n, bc, rhs[:n ** 3], ring[i % len(ring)][:n ** 3],
-                                        precision=prec, sweeps=args.sweeps))
-            for i in range(max(0, count - len(ring)), count):
-                collect(i)
-            span = max(ends) - t0
-            per_rate.append({"rate_req_s": rate, "p50_ms": float(np.percentile(lat, 50)),
-                             "p99_ms": float(np.percentile(lat, 99)), "throughput_req_s": count / span,
-                             "Mpoints_s": pts / span / 1e6, "refined_fraction": sum(used) / count})
-        st = S.stats()
-        S.close()
-        out[name] = {"per_rate": per_rate, "max_inflight": st["max_inflight"]}
+                    S.wait(wt[i - len(ring)])
+                wt.append(S.submit(n, n, n, bc, rhs[:n ** 3], ring[i % len(ring)][:n ** 3], precision=prec,
+                                   sweeps=args.sweeps))
+            for t in wt[max(0, count - len(ring)):]:
+                S.wait(t)
+            per_rate = []
+            for rate in SERVE_RATES:
+                arr = np.cumsum(np.random.default_rng(11 + rate).exponential(1.0 / rate, count))
+                tickets, t_sub = [], []
+                lat, ends, used = [0.0] * count, [0.0] * count, [0] * count
+                st0 = S.stats()
+                t0 = time.perf_counter()
+
+                def collect(i):
+                    st, ms, pu = S.wait(tickets[i])
+                    if st != 0:
+                        raise RuntimeError(f"request {i} failed with status {st}")
+                    lat[i] = (t_sub[i] - (t0 + arr[i])) * 1e3 + ms
+                    ends[i] = t_sub[i] + ms / 1e3
+                    used[i] = pu
+
+                for i, (n, bc) in enumerate(reqs):
+                    while time.perf_counter() < t0 + arr[i]:
+                        pass
+                    if i >= len(ring):
+                        collect(i - len(ring))
+                    t_sub.append(time.perf_counter())
+                    tickets.append(S.submit(n, n, n, bc, rhs[:n ** 3], ring[i % len(ring)][:n ** 3],
+                                            precision=prec, sweeps=args.sweeps))
+                for i in range(max(0, count - len(ring)), count):
+                    collect(i)
+                span = max(ends) - t0
+                st1 = S.stats()
+                per_rate.append({"rate_req_s": rate, "p50_ms": float(np.percentile(lat, 50)),
+                                 "p99_ms": float(np.percentile(lat, 99)), "throughput_req_s": count / span,
+                                 "Mpoints_s": pts / span / 1e6, "refined_fraction": sum(used) / count,
+                                 "handles_created": st1["handles_created"] - st0["handles_created"],
+                                 "handles_evicted": st1["handles_evicted"] - st0["handles_evicted"]})
+            st = S.stats()
+            S.close()
+            out[name][output] = {"per_rate": per_rate, "max_inflight": st["max_inflight"],
+                                 "handles_created": st["handles_created"], "handles_evicted": st["handles_evicted"]}
     return {"workload": f"{count} requests per rate (seed 11), cubic grids with log-uniform edge 32..384 "
                         "rounded to even 2/3/5-smooth, x/y family uniform, z DD, RHS N(0,1); 8 streams; "
-                        "latency from scheduled arrival to solution in host memory",
+                        "latency from scheduled arrival to solution in host memory; output the complex P "
+                        "or its real part alone",
             "rates_req_s": SERVE_RATES, "modes": out}
 
 

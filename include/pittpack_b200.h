@@ -242,7 +242,11 @@ typedef struct {
     int precision;     /* PP_PRECISION_FP64, or PP_PRECISION_MIXED (refined) */
     int sweeps;        /* refinement sweeps of the mixed mode */
     const double* rhs; /* host, real, nx*ny*nz doubles; page-locked for overlap */
-    double* P;         /* host, 2*nx*ny*nz doubles, written when the request completes */
+    double* P;         /* host, written when the request completes: 2*nx*ny*nz doubles
+                        * (complex P, chunkedArray layout), or nx*ny*nz doubles, the
+                        * solution's real part, when output_real is 1 */
+    int output_real;   /* 0: complex P; 1: the real part alone (half the copy; the
+                        * RHS is real, so the imaginary part is zero) */
 } pp_request;
 typedef struct pp_server_s* pp_server;
 /* 'streams' requests can be on the GPU at once; handles (plans, twiddles and

@@ -39,6 +39,7 @@ class Request(ctypes.Structure):
         ("sweeps", ctypes.c_int),
         ("rhs", ctypes.c_void_p),
         ("P", ctypes.c_void_p),
+        ("output_real", ctypes.c_int),
     ]
 
 
@@ -129,10 +130,12 @@ class Server:
 
     def submit(self, nx, ny, nz, bc, rhs: np.ndarray, P: np.ndarray, precision=0, sweeps=1,
                box=(0, 1, 0, 1, 0, 1)) -> int:
+        """Queue one solve; P is complex128 (the chunkedArray P) or float64 (the
+        solution's real part alone, half the copy), nx*ny*nz values."""
         if not (rhs.dtype == np.float64 and rhs.size == nx * ny * nz and rhs.flags.c_contiguous):
             raise ValueError("rhs must be contiguous float64 with nx*ny*nz values")
-        if not (P.dtype == np.complex128 and P.size == nx * ny * nz and P.flags.c_contiguous):
-            raise ValueError("P must be contiguous complex128 with nx*ny*nz values")
+        if not (P.dtype in (np.complex128, np.float64) and P.size == nx * ny * nz and P.flags.c_contiguous):
+            raise ValueError("P must be contiguous complex128 (or float64: real part) with nx*ny*nz values")
         r = Request()
         r.nx, r.ny, r.nz = nx, ny, nz
         r.bc = bc.encode()
@@ -141,6 +144,7 @@ class Server:
         r.sweeps = int(sweeps)
         r.rhs = rhs.ctypes.data
         r.P = P.ctypes.data
+        r.output_real = 1 if P.dtype == np.float64 else 0
         t = ctypes.c_ulonglong()
         check(self._L.pp_server_submit(self._h, ctypes.byref(r), ctypes.byref(t)), "pp_server_submit")
         self._keep[t.value] = (rhs, P)  # the buffers stay alive until wait()

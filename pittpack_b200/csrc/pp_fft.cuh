@@ -1,5 +1,8 @@
-// Batched mixed-radix (2,3,4,5,8) Stockham FFT on lines held in shared memory,
-// in FP64 (double2) or FP32 (float2).
+// Batched mixed-radix Stockham FFT on lines held in shared memory, in FP64
+// (double2) or FP32 (float2): register butterflies of radix 2, 3, 4, 5, 7
+// and 8, and one pass per remaining prime factor p, whose p-point DFTs are
+// summed directly (p^2 multiplies, twiddles from the line's own table), so
+// that every line length has a plan.
 //
 // The reference hands every line to FFTW or cuFFT (src/poissonCPU.cpp:40-234,
 // src/poissonGPU.cpp:5-97: unnormalised, exp(-2 pi i jk/N) forward and
@@ -22,6 +25,32 @@ struct PPFftPlan {
     int radix[PP_FFT_MAXPASS];   // radix of every pass, product = n
     const double2* tw;           // W_n^m = exp(-2 pi i m / n), m < n
 };
+
+// the passes of a length: radix 8 while 8 divides, then 4, 2, 3, 5, 7, then
+// the remaining prime factors in increasing order; false if n < 1
+PP_HD bool pp_fft_plan(int n, PPFftPlan* P)
+{
+    int m = n, k = 0;
+    if (n < 1) return false;
+    const int small[6] = {8, 4, 2, 3, 5, 7};
+    for (int q = 0; q < 6; ++q)
+        while (m % small[q] == 0 && k < PP_FFT_MAXPASS) {
+            P->radix[k++] = small[q];
+            m /= small[q];
+        }
+    for (int p = 11; p * p <= m && k < PP_FFT_MAXPASS; p += 2)
+        while (m % p == 0 && k < PP_FFT_MAXPASS) {
+            P->radix[k++] = p;
+            m /= p;
+        }
+    if (m > 1 && k < PP_FFT_MAXPASS) {
+        P->radix[k++] = m;
+        m = 1;
+    }
+    P->n = n;
+    P->npass = k;
+    return m == 1;
+}
 
 // r-point DFTs in registers; SIGN = -1 forward, +1 backward
 template <int SIGN, typename C>
@@ -106,6 +135,64 @@ PP_D void dft8(C* v)
     v[7] = c_sub(e[3], o3);
 }
 
+// R-point DFT in registers by direct summation, W_R^m = tw[m * rstride]
+// (the line's own table, W_n^{n/R} = W_R)
+template <int R, int SIGN, typename C>
+PP_D void dft_direct(C* v, const C* __restrict__ tw, int rstride)
+{
+    C out[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        C acc = v[0];
+#pragma unroll
+        for (int q = 1; q < R; ++q) {
+            C w = __ldg(&tw[((q * k) % R) * rstride]);
+            if (SIGN > 0) w.y = -w.y;
+            acc = c_add(acc, c_mul(v[q], w));
+        }
+        out[k] = acc;
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) v[k] = out[k];
+}
+
+// a pass of any radix r (a prime factor above 7): one thread per butterfly,
+// each output summed directly from the r inputs in shared memory
+template <int SIGN, typename C>
+PP_D void stockham_pass_any(const C* __restrict__ src, C* __restrict__ dst, int n, int nlines, int ns, int r,
+                            const C* __restrict__ tw, int tid, int nthreads)
+{
+    const int nb = n / r;
+    const int tstride = n / (ns * r);
+    const int total = nb * nlines;
+    for (int t = tid; t < total; t += nthreads) {
+        const int l = t / nb;
+        const int j = t - l * nb;
+        const int k = j % ns;
+        const C* in = src + l * n;
+        C* out = dst + l * n;
+        const int base = (j / ns) * ns * r + k;
+        for (int ko = 0; ko < r; ++ko) {
+            C acc = in[j];
+            int m = 0;  // q ko mod r
+            for (int q = 1; q < r; ++q) {
+                m += ko;
+                if (m >= r) m -= r;
+                C v = in[j + q * nb];
+                if (ns > 1) {
+                    C w = __ldg(&tw[q * k * tstride]);
+                    if (SIGN > 0) w.y = -w.y;
+                    v = c_mul(v, w);
+                }
+                C w = __ldg(&tw[m * nb]);
+                if (SIGN > 0) w.y = -w.y;
+                acc = c_add(acc, c_mul(v, w));
+            }
+            out[base + ko * ns] = acc;
+        }
+    }
+}
+
 template <int R, int SIGN, typename C>
 PP_D void stockham_pass(const C* __restrict__ src, C* __restrict__ dst, int n, int nlines, int ns,
                         const C* __restrict__ tw, int tid, int nthreads)
@@ -134,6 +221,7 @@ PP_D void stockham_pass(const C* __restrict__ src, C* __restrict__ dst, int n, i
         if (R == 3) dft3<SIGN>(v);
         if (R == 4) dft4<SIGN>(v);
         if (R == 5) dft5<SIGN>(v);
+        if (R == 7) dft_direct<7, SIGN>(v, tw, nb);
         if (R == 8) dft8<SIGN>(v);
         const int base = (j / ns) * ns * R + k;
 #pragma unroll
@@ -159,7 +247,9 @@ __device__ C* fft_lines(C* a, C* b, int nlines, const PPFftPlan& P, const C* tw,
         case 3: stockham_pass<3, SIGN>(src, dst, P.n, nlines, ns, tw, tid, nthreads); break;
         case 4: stockham_pass<4, SIGN>(src, dst, P.n, nlines, ns, tw, tid, nthreads); break;
         case 5: stockham_pass<5, SIGN>(src, dst, P.n, nlines, ns, tw, tid, nthreads); break;
-        default: stockham_pass<8, SIGN>(src, dst, P.n, nlines, ns, tw, tid, nthreads); break;
+        case 7: stockham_pass<7, SIGN>(src, dst, P.n, nlines, ns, tw, tid, nthreads); break;
+        case 8: stockham_pass<8, SIGN>(src, dst, P.n, nlines, ns, tw, tid, nthreads); break;
+        default: stockham_pass_any<SIGN>(src, dst, P.n, nlines, ns, r, tw, tid, nthreads); break;
         }
         __syncthreads();
         C* t = src;

@@ -83,7 +83,7 @@ cudaError_t pp_launch_line_pass_mixed_f32(const PPLinePassArgs& a, bool inverse,
 // 9 2^k and 15 2^k (144 .. 1152), called by the two above
 cudaError_t pp_launch_line_pass_mixed915(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st);
 cudaError_t pp_launch_line_pass_mixed915_f32(const PPLinePassArgs& a, bool inverse, bool strided, cudaStream_t st);
-// generic 2/3/5-smooth lengths; fp32: the FP32 kernel, twiddles from a.tw and
+// every other length (pp_fft_plan); fp32: the FP32 kernel, twiddles from a.tw and
 // a.cs2 (FP64: a.fft.tw and a.cs), with the refinement epilogue when a.acc is set
 cudaError_t pp_launch_line_pass(const PPLinePassArgs& a, bool inverse, bool strided, bool in_cplx, bool out_cplx,
                                 cudaStream_t st, bool fp32 = false);

@@ -71,20 +71,6 @@ int na_kind(char lo, char hi)
     return -1;
 }
 
-bool na_radix(int n, PPFftPlan& P)
-{
-    int m = n, k = 0;
-    auto push = [&](int r) { P.radix[k++] = r; m /= r; };
-    while (m % 8 == 0 && k < PP_FFT_MAXPASS) push(8);
-    while (m % 4 == 0 && k < PP_FFT_MAXPASS) push(4);
-    while (m % 2 == 0 && k < PP_FFT_MAXPASS) push(2);
-    while (m % 3 == 0 && k < PP_FFT_MAXPASS) push(3);
-    while (m % 5 == 0 && k < PP_FFT_MAXPASS) push(5);
-    P.n = n;
-    P.npass = k;
-    return m == 1;
-}
-
 // one direction of the solve: its length, family and FFT plan
 struct NaDir {
     int n = 0, nf = 0, kind = -1;
@@ -98,7 +84,9 @@ int na_dir(NaDir& d, int n, int kind)
     const bool quarter = pp_kind_is_quarter(kind);
     if (quarter && n % 2) return PP_UNSUPPORTED;
     d.nf = quarter ? n / 2 : n;
-    return na_radix(d.nf, d.fft) ? PP_SUCCESS : PP_UNSUPPORTED;
+    if (!pp_fft_plan(d.nf, &d.fft)) return PP_UNSUPPORTED;
+    if (pp_lp2_lpc(n) == 0 && pp_lpm_lpc(n) == 0 && pp_line_pass_smem(1, d.nf) > 227 * 1024) return PP_UNSUPPORTED;
+    return PP_SUCCESS;
 }
 
 int na_tag_xy(int kind) { return kind == PP_KIND_DST2 ? 0 : kind == PP_KIND_DCT2 ? 1 : kind == PP_KIND_FFT ? 2 : -1; }

@@ -213,7 +213,7 @@ bool admit(pp_server_s* S, const Req& q)
     if (rc == PP_SUCCESS) rc = pp_set_stream(h, s.stream);
     if (rc == PP_SUCCESS) rc = pp_assign_rhs_async(h, r.rhs);
     if (rc == PP_SUCCESS) rc = pp_solve(h);
-    if (rc == PP_SUCCESS) rc = pp_get_solution_async(h, r.P);
+    if (rc == PP_SUCCESS) rc = r.output_real ? pp_get_solution_real_async(h, r.P) : pp_get_solution_async(h, r.P);
     if (rc != PP_SUCCESS) {
         fail(S, q.ticket, rc);
         return true;
@@ -293,7 +293,7 @@ extern "C" int pp_server_submit(pp_server S, const pp_request* r, unsigned long 
 {
     if (!S) return PP_INVALID_HANDLE;
     if (!r || !ticket || !r->rhs || !r->P || r->nx < 2 || r->ny < 2 || r->nz < 3) return PP_INPUT_ARGS;
-    if (r->sweeps < 0 || r->sweeps > 16) return PP_INPUT_ARGS;
+    if (r->sweeps < 0 || r->sweeps > 16 || (r->output_real != 0 && r->output_real != 1)) return PP_INPUT_ARGS;
     std::lock_guard<std::mutex> g(S->mu);
     if (S->stop) return PP_NOT_READY;
     const unsigned long long t = S->next_ticket++;

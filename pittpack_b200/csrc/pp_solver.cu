@@ -27,18 +27,13 @@ int kind_from_bc(char lo, char hi)
     return -1;
 }
 
-// factor n into the radices of the Stockham passes; false if n has a prime
-// factor above 5
+// factor n into the radices of the Stockham passes (pp_fft_plan: every length)
 bool radix_plan(int n, std::vector<int>& r)
 {
-    r.clear();
-    int m = n;
-    while (m % 8 == 0) { r.push_back(8); m /= 8; }
-    while (m % 4 == 0) { r.push_back(4); m /= 4; }
-    while (m % 2 == 0) { r.push_back(2); m /= 2; }
-    while (m % 3 == 0) { r.push_back(3); m /= 3; }
-    while (m % 5 == 0) { r.push_back(5); m /= 5; }
-    return m == 1 && (int)r.size() <= PP_FFT_MAXPASS;
+    PPFftPlan P{};
+    const bool ok = pp_fft_plan(n, &P);
+    r.assign(P.radix, P.radix + P.npass);
+    return ok;
 }
 
 struct DevBuf {
@@ -133,6 +128,10 @@ int build_dir(pp_solver_s* h, DirTables& t, int n, int kind)
     const int nf = quarter ? n / 2 : n;
     std::vector<int> r;
     if (!radix_plan(nf, r)) return PP_UNSUPPORTED;
+    // the generic kernel holds a tile of at least one line (two buffers) in
+    // shared memory: lengths past that limit, outside the register kernels,
+    // are not taken
+    if (pp_lp2_lpc(n) == 0 && pp_lpm_lpc(n) == 0 && pp_line_pass_smem(1, nf) > 227 * 1024) return PP_UNSUPPORTED;
     t.fft.n = nf;
     t.fft.npass = (int)r.size();
     for (size_t i = 0; i < r.size(); ++i) t.fft.radix[i] = r[i];

@@ -65,7 +65,9 @@ def test_server_submit_checks_host_buffers():
     with pytest.raises(ValueError):
         S.submit(4, 4, 4, "NNNNDD", np.zeros(n - 1), np.zeros(n, dtype=np.complex128))
     with pytest.raises(ValueError):
-        S.submit(4, 4, 4, "NNNNDD", np.zeros(n), np.zeros(n, dtype=np.float64))
+        S.submit(4, 4, 4, "NNNNDD", np.zeros(n), np.zeros(n, dtype=np.float32))  # complex128 or float64 only
+    with pytest.raises(ValueError):
+        S.submit(4, 4, 4, "NNNNDD", np.zeros(n), np.zeros(n - 1, dtype=np.float64))
     assert S._keep == {}
 
 

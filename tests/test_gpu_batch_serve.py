@@ -104,6 +104,32 @@ def test_server_results_same_alone_and_in_the_mix():
     S.close()
 
 
+def test_server_real_part_output_in_the_mix():
+    """Requests asking for the solution's real part alone (half the copy)
+    mixed with requests for the complex P: each real-part result is exactly the
+    real part of the same request's complex result."""
+    from pittpack_b200.batch import Server
+    from pittpack_b200.poisson import pinned_empty
+
+    grids = _grids(13, 12)
+    S = Server(streams=4, hbm_fraction=0.3)
+    pairs = []
+    for k, (nx, ny, nz, bc, f) in enumerate(grids):
+        rhs = pinned_empty(f.shape, np.float64)
+        rhs[...] = f
+        Pc = pinned_empty(f.shape, np.complex128)
+        Pr = pinned_empty(f.shape, np.float64)
+        prec = k % 2
+        pairs.append((S.submit(nx, ny, nz, bc, rhs, Pc, precision=prec, sweeps=2),
+                      S.submit(nx, ny, nz, bc, rhs, Pr, precision=prec, sweeps=2), Pc, Pr, rhs))
+    for tc, tr, Pc, Pr, _ in pairs:
+        assert S.wait(tc)[0] == 0 and S.wait(tr)[0] == 0
+        assert np.array_equal(np.asarray(Pr), np.asarray(Pc).real)
+    st = S.stats()
+    assert st["handles_created"] >= 1 and st["handles_evicted"] >= 0
+    S.close()
+
+
 def test_server_rejects_a_request_that_never_fits():
     from pittpack_b200.batch import Server
     from pittpack_b200.poisson import pinned_empty

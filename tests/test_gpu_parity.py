@@ -73,7 +73,9 @@ def test_all_families_vs_oracle(bcx, bcy, bcz, shape):
 
 
 @pytest.mark.parametrize("shape", [(30, 48, 20), (96, 10, 7), (12, 160, 33), (64, 64, 3), (2, 6, 4), (50, 45, 4),
-                                   (128, 96, 100), (16, 2048, 5), (1024, 16, 9), (256, 128, 64)])
+                                   (128, 96, 100), (16, 2048, 5), (1024, 16, 9), (256, 128, 64),
+                                   # lengths with prime factors above 5 (radix-7 passes, direct prime passes)
+                                   (14, 97, 6), (112, 22, 9), (97, 61, 5), (26, 7, 12), (251, 18, 4), (98, 17, 5)])
 @pytest.mark.parametrize("bc", ["NNDDNN", "PPPPDD", "DDNNPP", "DNPPDN", "NDDDND"])
 def test_sizes_vs_oracle(shape, bc):
     nx, ny, nz = shape
@@ -163,5 +165,5 @@ def test_errors_are_returned_not_fatal():
         with pytest.raises(pp.PittPackError):
             M.pittPack()  # no RHS yet
     with pytest.raises(pp.PittPackError) as e:
-        pp.make_Poisson(14, 8, 8).assignBoundary("DDDDDD")  # 14 = 2 * 7: no radix-7 pass
+        pp.make_Poisson(15, 8, 8).assignBoundary("NDDDDD")  # the quarter-wave N-D family needs an even length
     assert e.value.code == 27

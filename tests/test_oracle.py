@@ -150,3 +150,27 @@ def test_oracle_equals_the_reference_build_on_every_family(bc):
         Q = O.solve(O.problem(nx, ny, nz, bc, tuple(box)), fr, fi)
         # identical bits on this image; the bound allows another libm
         assert O.rel_l2(Q, out.view(np.complex128).reshape(nz, ny, nx)) <= 1e-15, (bc, (nx, ny, nz))
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference build absent (make -C oracle)")
+@pytest.mark.parametrize("shape", [(14, 13, 5), (7, 22, 6), (11, 17, 4), (26, 9, 7)])
+@pytest.mark.parametrize("bc", ["PPPPDD", "NNNNDD", "DDDDNN", "NNDDPP"])
+def test_oracle_equals_the_reference_build_on_lengths_with_large_prime_factors(bc, shape):
+    """Lengths with prime factors above 5 (7, 11, 13, 17): the reference
+    hands them to FFTW like any other; the oracle's DFT takes every length."""
+    import ctypes
+
+    L = ctypes.CDLL(REF_LIB)
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.ppref_solve.argtypes = [ctypes.c_int] * 3 + [ctypes.c_char_p, dp, dp, dp, dp, dp]
+    nx, ny, nz = shape
+    rng = np.random.default_rng(nx * ny + nz)
+    fr = rng.uniform(-1, 1, (nz, ny, nx))
+    fi = rng.uniform(-1, 1, (nz, ny, nx)) if bc[0] == "P" else None
+    out = np.zeros(2 * nx * ny * nz)
+    box = np.array([0, 1, 0, 1, 0, 1.0])
+    sec = ctypes.c_double()
+    L.ppref_solve(nx, ny, nz, bc.encode(), box.ctypes.data_as(dp), fr.ctypes.data_as(dp),
+                  None if fi is None else fi.ctypes.data_as(dp), out.ctypes.data_as(dp), ctypes.byref(sec))
+    Q = O.solve(O.problem(nx, ny, nz, bc), fr, fi)
+    assert O.rel_l2(Q, out.view(np.complex128).reshape(nz, ny, nx)) <= 1e-15, (bc, shape)
