@@ -555,6 +555,15 @@ __device__ __forceinline__ void lp2_body(const PPLinePassArgs& a)
                 emit(kk, Zk, ln[rp_pad(N - kk)]);
             }
         }
+        // the rows of the half spectra are padded to the y pass's tile width:
+        // the padding columns are zeroed, since the y pass of a real family
+        // transforms two columns as one complex line and a column's partner
+        // must not carry stale values into it
+        const int npad = (int)ols - (N / 2 + 1);
+        for (int idx = tid; idx < DL * npad; idx += NT) {
+            const int l = idx / npad, e = N / 2 + 1 + (idx - (idx / npad) * npad);
+            if (l < nl) put<Real>(a, goff(l, e), plane, (Real)0, (Real)0, sc);
+        }
     } else if constexpr (C2R) {
         // z = x_a + i x_b: both real lines at once
         constexpr int LL = rp_log2(LPC);
