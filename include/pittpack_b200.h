@@ -186,6 +186,11 @@ int pp_fill_trigonometric_box(int nx, int ny, int nz, const double box[6], doubl
  * whose MultiGrid prints its residuals (src/multiGrid.cpp:1415-1515) */
 int pp_zsolve_stats(pp_handle h, int* max_cycles, int* unconverged);
 
+/* thread blocks of this handle's transform passes whose bounded wait for
+ * their bulk-copied tile ran out (each left without output, so the solve is
+ * wrong if this is not 0); waits for the handle's stream.  No counterpart in
+ * the reference. */
+int pp_kernel_timeouts(pp_handle h, int* count);
 /* CUDA stream for the handle's work (cudaStream_t passed as void*); 0 = legacy */
 int pp_set_stream(pp_handle h, void* stream);
 int pp_synchronize(pp_handle h);

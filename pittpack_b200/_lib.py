@@ -91,6 +91,7 @@ def load():
         "pp_assign_rhs_async": ([H, ctypes.c_void_p], i),
         "pp_get_solution_async": ([H, ctypes.c_void_p], i),
         "pp_get_solution_real": ([H, ctypes.c_void_p], i),
+        "pp_kernel_timeouts": ([H, ctypes.POINTER(i)], i),
         "pp_get_solution_real_async": ([H, ctypes.c_void_p], i),
         "pp_bind_device_buffers": ([H, ctypes.c_void_p, i, ctypes.c_void_p], i),
         "pp_set_tuning": ([H, ctypes.POINTER(Tuning)], i),

@@ -63,6 +63,9 @@ struct PPLinePassArgs {
     const double* zplane;
     double zscale;      // zplane[plane] is multiplied by this
     int acc_read;       // 0: the previous u is zero (first sweep), acc is not read
+    // bounded waits (the bulk-copy staging of the contiguous passes): a CTA
+    // whose wait runs out adds 1 here (if set) and returns without output
+    int* err;
 };
 
 // shared memory of the generic kernel: two buffers of L lines of nfft complex

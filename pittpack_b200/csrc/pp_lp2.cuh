@@ -123,6 +123,43 @@ PP_D void cp_async(void* smem, const void* gmem)
     if (BYTES == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 
+// ---- bulk-copy staging (the copy engine, not the LSU pipe) --------------------------
+PP_D unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// mbarrier with one arrival, armed for 'bytes' of bulk copies
+PP_D void mbar_init(unsigned bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+PP_D void mbar_expect(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+// global -> shared bulk copy (both addresses 16-byte aligned, bytes a
+// multiple of 16), completion counted on the mbarrier
+PP_D void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+// wait for phase 0 of the mbarrier, at most 'limit' polls; true if it completed
+PP_D bool mbar_wait0(unsigned bar, long limit)
+{
+    for (long i = 0; i < limit; ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 // row pitch (elements) of the strided pass's raw tile [element][line]: the
 // smallest pitch above the tile's line count whose rows start on 16-byte
 // boundaries and are an odd number of 16-byte units apart, so that threads
@@ -248,7 +285,28 @@ __device__ __forceinline__ void lp2_body(const PPLinePassArgs& a)
     constexpr int RUN = STRIDED ? DL : LLEN;         // elements per contiguous run
     constexpr int PER = 16 / (int)sizeof(RE);        // elements per 16-byte chunk
     constexpr bool VOK = (RUN * (int)sizeof(RE)) % 16 == 0;  // runs are whole chunks
-    if (VOK && same && a.vec16 && nl == DL) {
+    if (!STRIDED && VOK && same && a.vec16 && nl == DL) {
+        // contiguous pass, full tile of whole 16-byte lines: one bulk copy per
+        // line, issued by one thread and counted on an mbarrier, so that the
+        // staged bytes skip the LSU pipe the rest of the pass is bound by
+        __shared__ __align__(8) unsigned long long bulk_bar;
+        const unsigned bar = smem_u32(&bulk_bar);
+        constexpr unsigned LB = (unsigned)(LLEN * sizeof(RE));
+        if (tid == 0) mbar_init(bar);
+        __syncthreads();
+        if (tid == 0) {
+            mbar_expect(bar, LB * DL);
+            const RE* src = reinterpret_cast<const RE*>(a.src);
+            for (int r = 0; r < DL; ++r) bulk_g2s(raw + r * LLEN, src + base + (long)r * a.line_stride, LB, bar);
+        }
+        // a bounded wait (about a second of polls): a CTA whose copies never
+        // land counts itself and leaves without output, with every thread
+        const bool landed = mbar_wait0(bar, 1L << 22);
+        if (__syncthreads_or(!landed)) {
+            if (tid == 0 && a.err) atomicAdd(a.err, 1);
+            return;
+        }
+    } else if (VOK && same && a.vec16 && nl == DL) {
         constexpr int CPR = VOK ? RUN / PER : 1;     // chunks per run
         constexpr int TOT = (STRIDED ? LLEN : DL) * CPR;
         const RE* src = reinterpret_cast<const RE*>(a.src);

@@ -87,6 +87,7 @@ struct pp_solver_s {
     pp_tuning tune{0, 0, 0};  // launch-shape choices (0 = built-in default)
     DevBuf psum;   // refined solve: per-plane sums / zero-mode column (nz doubles)
     DevBuf part;   // refined solve: per-CTA partial sums of r and of u (2 x nz x tiles)
+    DevBuf errc;   // CTAs whose bounded waits ran out (one int)
     DevBuf zero1;  // one double 0.0 (eigen table of the zero-mode system)
     DevBuf mgstats;  // multigrid z solve: max cycles, unconverged systems (2 ints)
     DevBuf zmean;    // zero-mean option: partial sums and the mean
@@ -543,6 +544,7 @@ int launch_solve(pp_solver_s* h)
     ax.nz = nz;
     ax.dz = dz;
     ax.out_scale = 1.0;
+    ax.err = h->errc.as<int>();
 
     PPLinePassArgs ay = ax;
     ay.n = ny;
@@ -731,6 +733,7 @@ int launch_mixed(pp_solver_s* h)
     ax.nz = nz;
     ax.dz = dz;
     ax.out_scale = 1.0;
+    ax.err = h->errc.as<int>();
     PPLinePassArgs ay = ax;
     ay.n = ny;
     ay.kind = ky;
@@ -911,12 +914,14 @@ int pp_create(int nx, int ny, int nz, pp_handle* out)
     pp_default_options(&h->opt);
     const size_t n = (size_t)nx * ny * nz;
     if (h->rhs.alloc(2 * n * sizeof(double)) != cudaSuccess || h->bufA.alloc(2 * n * sizeof(double)) != cudaSuccess ||
-        h->bufB.alloc(2 * n * sizeof(double)) != cudaSuccess || h->out.alloc(2 * n * sizeof(double)) != cudaSuccess) {
+        h->bufB.alloc(2 * n * sizeof(double)) != cudaSuccess || h->out.alloc(2 * n * sizeof(double)) != cudaSuccess ||
+        h->errc.alloc(sizeof(int)) != cudaSuccess || cudaMemset(h->errc.p, 0, sizeof(int)) != cudaSuccess) {
         // release what did fit (the buffers have no destructor)
         h->rhs.free();
         h->bufA.free();
         h->bufB.free();
         h->out.free();
+        h->errc.free();
         cudaGetLastError();
         delete h;
         return PP_ALLOCATION_FAIL;
@@ -939,6 +944,7 @@ int pp_destroy(pp_handle h)
     timing_release(h);
     h->psum.free();
     h->part.free();
+    h->errc.free();
     h->zero1.free();
     h->mgstats.free();
     h->zmean.free();
@@ -1021,6 +1027,17 @@ int pp_set_options(pp_handle h, const pp_options* opt)
         return build_lift(h);
     }
     return PP_SUCCESS;
+}
+
+int pp_kernel_timeouts(pp_handle h, int* count)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!count) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    cudaSetDevice(h->device);
+    cudaError_t e = cudaMemcpyAsync(count, h->errc.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return e == cudaSuccess ? PP_SUCCESS : set_cuda_error(h, e, PP_CUDA_ERROR);
 }
 
 int pp_zsolve_stats(pp_handle h, int* max_cycles, int* unconverged)
@@ -1369,7 +1386,7 @@ int pp_workspace_bytes(pp_handle h, size_t* bytes)
     for (auto& l : h->lift) b += l.bytes;
     for (const DirTables* t : {&h->tx, &h->ty})
         b += t->tw.bytes + t->cs.bytes + t->eig.bytes + t->twf.bytes + t->csf.bytes;
-    b += h->psum.bytes + h->part.bytes + h->zero1.bytes + h->mgstats.bytes + h->zmean.bytes;
+    b += h->psum.bytes + h->part.bytes + h->errc.bytes + h->zero1.bytes + h->mgstats.bytes + h->zmean.bytes;
     *bytes = b;
     return PP_SUCCESS;
 }

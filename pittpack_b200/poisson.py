@@ -221,6 +221,13 @@ class PoissonGPU:
             raise PittPackError(_lib.PP_INPUT_ARGS, "getSolutionAsync needs a contiguous complex128 array of nx*ny*nz")
         check(self._L.pp_get_solution_async(self._h, out.ctypes.data), "pp_get_solution_async")
 
+    def kernelTimeouts(self) -> int:
+        """Thread blocks whose bounded wait for their bulk-copied tile ran out
+        (0 unless the copy engine failed; each such block wrote no output)."""
+        c = ctypes.c_int()
+        check(self._L.pp_kernel_timeouts(self._h, ctypes.byref(c)), "pp_kernel_timeouts")
+        return c.value
+
     def getSolutionReal(self, out: np.ndarray | None = None) -> np.ndarray:
         """The real part of the solution alone (float64, shape (nz, ny, nx)):
         half the bytes of getSolution, for a real RHS (whose solution has a

@@ -146,7 +146,29 @@ def test_repeat_solves_are_identical_and_rhs_reusable():
         a = M.getSolution()
         M.pittPack()
         b = M.getSolution()
+        # no block of the contiguous passes missed its bulk-copied tile
+        assert M.kernelTimeouts() == 0
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("bc", ["PPPPDD", "NNNNDD", "NDNDDD", "DDDDDD"])
+def test_bulk_copied_tiles_at_the_benchmark_length(bc):
+    """The contiguous passes stage full tiles with the copy engine (one bulk
+    copy per line, an mbarrier with a bounded wait): at 512 x 64 x 16 every
+    tile is full, the solution matches the oracle and no wait ran out."""
+    import pittpack_b200 as pp
+
+    nx, ny, nz = 512, 64, 16
+    f = np.random.default_rng(5).uniform(-1, 1, (nz, ny, nx))
+    with pp.make_Poisson(nx, ny, nz) as M:
+        M.assignBoundary(bc)
+        M.assignRhs(f)
+        for prec in (0, 1):
+            M.setOptions(precision=prec, compat_zero_mode=1 - prec)
+            M.pittPack()
+            Q = O.solve(O.problem(nx, ny, nz, bc, compat_zero_mode=1 - prec), f)
+            assert O.rel_l2(M.getSolution(), Q) <= (TOL if prec == 0 else 1e-10)
+        assert M.kernelTimeouts() == 0
 
 
 def test_errors_are_returned_not_fatal():
