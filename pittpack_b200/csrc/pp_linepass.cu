@@ -25,9 +25,11 @@
 //   DST-II/III (D-D): the same with swap x'[j] = (-1)^j x[N-1-j] before and
 //           after (:202-265).
 //   FFT     (P-P): the plain unnormalised DFT.
-//   DCT-IV / DST-IV (N-D / D-N, not in the reference): N/2-point complex FFT
-//           of z_m = (x_{2m} + i x_{N-1-2m}) e^{-i pi m/N}, then
-//           w_p = e^{-i pi (4p+1)/(4N)} Z_p, X_{2p} = c Re w_p, X_{N-1-2p} = -c Im w_p
+//   DCT-IV / DST-IV (N-D / D-N, not in the reference): even N, an N/2-point
+//           complex FFT of z_m = (x_{2m} + i x_{N-1-2m}) e^{-i pi m/N}, then
+//           w_p = e^{-i pi (4p+1)/(4N)} Z_p, X_{2p} = c Re w_p, X_{N-1-2p} = -c Im w_p;
+//           odd N, a 2N-point FFT of y_m = x_m e^{-i pi m/(2N)} (m < N, zero
+//           above), then X_k = c Re(e^{-i pi (2k+1)/(4N)} Y_k), k < N
 //           (c = 2 forward, 1 inverse); DST-IV reverses the input and flips
 //           the sign of odd outputs.
 // The DCT/DST families read only the real part of their input, as the
@@ -80,7 +82,8 @@ __global__ void __launch_bounds__(PP_LINE_THREADS) line_pass_kernel(PPLinePassAr
     const int n = a.n;
     const int kind = a.kind;
     const bool quarter = pp_kind_is_quarter(kind);
-    const int nf = a.fft.n;  // n, or n/2 for the quarter-wave families
+    const bool q_odd = quarter && (n & 1);  // quarter-wave, odd length: 2n-point FFT
+    const int nf = a.fft.n;  // n; n/2 (even) or 2n (odd) for the quarter-wave families
     const int tid = threadIdx.x;
     const int nth = blockDim.x;
     // FFT and family twiddles in the kernel's precision
@@ -163,7 +166,14 @@ __global__ void __launch_bounds__(PP_LINE_THREADS) line_pass_kernel(PPLinePassAr
             const int k = idx - l * nf;
             const R* X = stage + l * n;
             C V;
-            if (quarter) {
+            if (q_odd) {
+                if (k < n) {
+                    const C w = __ldg(&cs[k]);  // e^{-i pi k / (2n)}
+                    V = mkc<C>(X[k] * w.x, X[k] * w.y);
+                } else {
+                    V = mkc<C>((R)0, (R)0);
+                }
+            } else if (quarter) {
                 const C w = __ldg(&cs[k]);  // e^{-i pi k / n}
                 const R xa = X[2 * k], xb = X[n - 1 - 2 * k];
                 V = mkc<C>(xa * w.x - xb * w.y, xa * w.y + xb * w.x);
@@ -203,6 +213,13 @@ __global__ void __launch_bounds__(PP_LINE_THREADS) line_pass_kernel(PPLinePassAr
         C o;
         if (kind == PP_KIND_FFT) {
             o = Rl[e];
+        } else if (q_odd) {
+            const C w = __ldg(&cs[n + e]);  // e^{-i pi (2e+1)/(4n)}
+            const C z = Rl[e];
+            R v = z.x * w.x - z.y * w.y;
+            v *= INVERSE ? (R)1 : (R)2;
+            if (kind == PP_KIND_DST4 && (e & 1)) v = -v;
+            o = mkc<C>(v, (R)0);
         } else if (quarter) {
             const int k = e;
             const int p = (k & 1) == 0 ? (k >> 1) : ((n - 1 - k) >> 1);

@@ -81,9 +81,7 @@ int na_dir(NaDir& d, int n, int kind)
 {
     d.n = n;
     d.kind = kind;
-    const bool quarter = pp_kind_is_quarter(kind);
-    if (quarter && n % 2) return PP_UNSUPPORTED;
-    d.nf = quarter ? n / 2 : n;
+    d.nf = pp_fft_len(n, kind);
     if (!pp_fft_plan(d.nf, &d.fft)) return PP_UNSUPPORTED;
     if (pp_lp2_lpc(n) == 0 && pp_lpm_lpc(n) == 0 && pp_line_pass_smem(1, d.nf) > 227 * 1024) return PP_UNSUPPORTED;
     return PP_SUCCESS;
@@ -143,9 +141,10 @@ __global__ void na_tables_kernel(NaTables t)
                 t.tw[d][idx] = make_double2(c, sn);
             } else if (part == 1) {
                 if (pp_kind_is_quarter(kind)) {
+                    long num, den;
+                    pp_quarter_angle(n, idx, &num, &den);
                     double sn, c;
-                    if (idx < nf) sincospi(-(double)idx / n, &sn, &c);
-                    else sincospi(-(double)(4 * (idx - nf) + 1) / (4.0 * n), &sn, &c);
+                    sincospi(-(double)num / (double)den, &sn, &c);
                     t.cs[d][idx] = make_double2(c, sn);
                 } else {
                     t.cs[d][idx] = pp_family_twiddle(n, idx);
@@ -263,10 +262,10 @@ extern "C" int pp_solve_noalloc(int nx, int ny, int nz, const char bc[6], const 
         tb.nf[d] = dirs[d]->nf;
         tb.kind[d] = dirs[d]->kind;
         tb.tw[d] = cv.take<double2>(dirs[d]->nf);
-        tb.cs[d] = cv.take<double2>(dirs[d]->n);
+        tb.cs[d] = cv.take<double2>(pp_family_table_len(dirs[d]->n, dirs[d]->kind));
         tb.eig[d] = cv.take<double>(dirs[d]->n);
         tb.len[3 * d] = dirs[d]->nf;
-        tb.len[3 * d + 1] = dirs[d]->n;
+        tb.len[3 * d + 1] = pp_family_table_len(dirs[d]->n, dirs[d]->kind);
         tb.len[3 * d + 2] = dirs[d]->n;
     }
 

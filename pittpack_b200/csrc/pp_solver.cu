@@ -125,8 +125,7 @@ int build_dir(pp_solver_s* h, DirTables& t, int n, int kind)
     t.n = n;
     t.kind = kind;
     const bool quarter = pp_kind_is_quarter(kind);
-    if (quarter && (n % 2) != 0) return PP_UNSUPPORTED;
-    const int nf = quarter ? n / 2 : n;
+    const int nf = pp_fft_len(n, kind);
     std::vector<int> r;
     if (!radix_plan(nf, r)) return PP_UNSUPPORTED;
     // the generic kernel holds a tile of at least one line (two buffers) in
@@ -145,14 +144,13 @@ int build_dir(pp_solver_s* h, DirTables& t, int n, int kind)
     }
     std::vector<double2> cs;
     if (quarter) {
-        cs.resize(n);
-        for (int m = 0; m < nf; ++m) {
-            long double a = -pi_l * (long double)m / (long double)n;
+        // pre- and post-twiddles e^{-i pi num / den}
+        cs.resize(pp_family_table_len(n, kind));
+        for (size_t m = 0; m < cs.size(); ++m) {
+            long num, den;
+            pp_quarter_angle(n, (int)m, &num, &den);
+            long double a = -pi_l * (long double)num / (long double)den;
             cs[m] = make_double2((double)cosl(a), (double)sinl(a));
-        }
-        for (int p = 0; p < nf; ++p) {
-            long double a = -pi_l * (long double)(4 * p + 1) / (4.0L * n);
-            cs[nf + p] = make_double2((double)cosl(a), (double)sinl(a));
         }
     } else {
         cs.resize(n);

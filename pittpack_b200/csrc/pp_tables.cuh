@@ -98,3 +98,46 @@ PP_HD void pp_mms_face_dims(const PPMmsFaces& p, int slot, int* na, int* nb)
         *nb = p.nz;
     }
 }
+
+// FFT length of a direction.  The quarter-wave families (DCT-IV / DST-IV) of
+// even length n run one n/2-point complex FFT of the paired, pre-twiddled
+// line; of odd length n, one 2n-point FFT of the pre-twiddled line padded
+// with n zeros:
+//   X_k = c Re[ e^{-i pi (2k+1)/(4n)} sum_{m<n} (x_m e^{-i pi m/(2n)}) e^{-2 pi i m k/(2n)} ].
+// Every other family: n.
+PP_HD int pp_fft_len(int n, int kind)
+{
+    if (!pp_kind_is_quarter(kind)) return n;
+    return (n & 1) ? 2 * n : n / 2;
+}
+
+// entries of a direction's family-twiddle table: the DCT/DST families' n
+// (theta_k); the quarter-wave families' pre- and post-twiddles, n / 2 each
+// (even n) or n each (odd n)
+PP_HD int pp_family_table_len(int n, int kind) { return (pp_kind_is_quarter(kind) && (n & 1)) ? 2 * n : n; }
+
+// the quarter-wave families' twiddle table entry idx, as the fraction f of pi
+// in e^{-i pi f}: even n, idx < n/2: m / n (pre, m = idx), else
+// (4p + 1) / (4n) (post, p = idx - n/2); odd n, idx < n: m / (2n), else
+// (2k + 1) / (4n) (k = idx - n)
+PP_HD void pp_quarter_angle(int n, int idx, long* num, long* den)
+{
+    if (n & 1) {
+        if (idx < n) {
+            *num = idx;
+            *den = 2L * n;
+        } else {
+            *num = 2L * (idx - n) + 1;
+            *den = 4L * n;
+        }
+    } else {
+        const int h = n / 2;
+        if (idx < h) {
+            *num = idx;
+            *den = n;
+        } else {
+            *num = 4L * (idx - h) + 1;
+            *den = 4L * n;
+        }
+    }
+}

@@ -65,6 +65,7 @@ def test_noalloc_matches_handle_path_and_oracle_on_calls_in_a_row():
         (128, 64, 32, "PPPPDN", (0, 2, 0, 1, 0.5, 1.5)),  # power-of-two lengths, periodic x/y
         (256, 256, 16, "NNNNDD", (0, 1, 0, 1, 0, 1)),     # >= 256^2 z systems, 16 rows per lane
         (256, 256, 20, "DDNNDD", (0, 1, 0, 1, 0, 1)),     # >= 256^2 z systems, uneven register rows
+        (45, 21, 12, "NDDNDD", (0, 1, 0, 1, 0, 1)),      # odd quarter-wave lengths: 2n-point FFTs
     ]
     inputs = [rng.uniform(-1, 1, (nz, ny, nx)) for nx, ny, nz, _, _ in cases]
     first = None
