@@ -8,7 +8,6 @@
 
 #define PP_LINE_THREADS 256
 #define PP_Z_THREADS 256
-#define PP_Z_MAX_NZ 4096
 
 // Dirichlet face corrections subtracted from the dz^2-scaled RHS
 // (modifyRhsDirichlet, src/pencilDcmp.cpp:4623-4835); null where a face is
@@ -124,6 +123,11 @@ void pp_zsolve_config(int nz, bool cplx, int nx, int* TS, int* threads);
 void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* threads, int systems = 0, int ny = 0);
 int pp_zsolve_valid_lanes(int nz, int P);
 size_t pp_zsolve_smem_p(int TS, int nz, bool cplx, int P);
+// the longest z systems the z solve takes: a CTA of one system on 32 lanes
+// whose column, pivot table and scratch fit the opt-in shared memory of a
+// CTA (cplx: complex spectra; g32: the refined solve's FP32 spectra, staged
+// beside the tile); about 25,000 rows for real spectra, 13,000 for complex
+int pp_zsolve_max_nz(bool cplx, bool g32);
 
 // FP64 residual r = f dz^2 - lift - A u of the refined solve (pp_mixed.cu)
 struct PPResidArgs {

@@ -238,7 +238,7 @@ extern "C" int pp_solve_noalloc(int nx, int ny, int nz, const char bc[6], const 
     if (kx < 0 || ky < 0 || (bc[4] == 'P') != (bc[5] == 'P')) return PP_INPUT_ARGS;
     for (int d = 0; d < 3; ++d)
         if (!(box[2 * d + 1] > box[2 * d])) return PP_INPUT_ARGS;
-    if (nz > PP_Z_MAX_NZ) return PP_UNSUPPORTED;
+    if (nz > pp_zsolve_max_nz(ky == PP_KIND_FFT, false)) return PP_UNSUPPORTED;
 
     NaDir tx, ty;
     int rc;

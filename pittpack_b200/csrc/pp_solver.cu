@@ -310,6 +310,9 @@ int valid_bc(const char* bc)
 
 int rebuild_tables(pp_solver_s* h)
 {
+    // complex spectra (periodic y) make the z solve's column twice as long
+    if (kind_from_bc(h->bc[2], h->bc[3]) == PP_KIND_FFT && h->nz > pp_zsolve_max_nz(true, false))
+        return PP_UNSUPPORTED;
     int rc = build_dir(h, h->tx, h->nx, kind_from_bc(h->bc[0], h->bc[1]));
     if (rc != PP_SUCCESS) return rc;
     rc = build_dir(h, h->ty, h->ny, kind_from_bc(h->bc[2], h->bc[3]));
@@ -681,6 +684,7 @@ int launch_mixed(pp_solver_s* h)
     cudaError_t e;
     int t0;
     if (h->rhs_complex || h->opt.z_solver != PP_ZSOLVE_DIRECT) return PP_UNSUPPORTED;
+    if (nz > pp_zsolve_max_nz(s_cplx, true)) return PP_UNSUPPORTED;  // FP32 spectra staged beside the tile
     // singular: no Dirichlet end anywhere (the x/y families with a zero mode
     // are N-N or P-P)
     const bool singular = zm && h->bc[4] != 'D' && h->bc[5] != 'D';
@@ -900,7 +904,7 @@ int pp_create(int nx, int ny, int nz, pp_handle* out)
     if (!out) return PP_INPUT_ARGS;
     *out = nullptr;
     if (nx < 2 || ny < 2 || nz < 3) return PP_INPUT_ARGS;
-    if (nz > PP_Z_MAX_NZ) return PP_UNSUPPORTED;
+    if (nz > pp_zsolve_max_nz(false, false)) return PP_UNSUPPORTED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PP_GPU_INIT_FAILURE;
     pp_solver_s* h = new (std::nothrow) pp_solver_s;

@@ -671,9 +671,20 @@ void pp_zsolve_config_p(int nz, bool cplx, int nx, int lanes, int* TS, int* thre
     *threads = ts * P < 32 ? 32 : ts * P;
 }
 
+int pp_zsolve_max_nz(bool cplx, bool g32)
+{
+    int lo = 3, hi = 1 << 16;  // lo fits, hi does not
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (zlayout(1, mid, 32, cplx, 32, g32).bytes <= (size_t)227 * 1024) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
 {
-    if (a0.nz < 3 || a0.nz > PP_Z_MAX_NZ) return cudaErrorInvalidValue;
+    if (a0.nz < 3 || a0.nz > pp_zsolve_max_nz(cplx, a0.data_fp32 != 0)) return cudaErrorInvalidValue;
     PPZArgs a = a0;
     const bool large = pp_zsolve_large((long)a.nx * a.ny);
     if (!pp_zsolve_valid_lanes(a.nz, a.P)) a.P = pp_zsolve_lanes(a.nz, cplx, large);

@@ -86,6 +86,33 @@ def test_sizes_vs_oracle(shape, bc):
     assert O.rel_l2(P, Q) <= TOL
 
 
+@pytest.mark.parametrize("nx,ny,nz,bc", [(4, 6, 6000, "NNDDDD"), (6, 4, 12000, "DDNNNN"), (8, 4, 5000, "PPPPDD"),
+                                         (4, 8, 9000, "NDPPPP")])
+def test_long_z_systems_vs_oracle(nx, ny, nz, bc):
+    """z systems past 4096 rows: one system per CTA on 32 lanes, its column
+    in shared memory; plain FP64 against the oracle, and the refined solve
+    against the oracle's exact-zero-mode solution for the real families.
+    Unit cells (a box of nx x ny x nz), so that the z systems of the
+    transverse modes keep the conditioning of a cubic cell grid.  The
+    periodic family's kx = ky = 0 column is the 1-D Dirichlet Laplacian of nz
+    rows (condition number about 0.4 nz^2, 1e7 at nz = 5000) and dominates the
+    solution: the partition method here and the serial Thomas sweep of the
+    oracle differ there by rounding amplified by that condition number (the
+    oracle's own solution leaves a 7-point residual of 1.4e-12 there), so
+    that case is held to 1e-11 (measured 3e-12)."""
+    rng = np.random.default_rng(nz)
+    f = rng.standard_normal((nz, ny, nx))
+    box = (0, nx, 0, ny, 0, nz)
+    Q = O.solve(O.problem(nx, ny, nz, bc, box=box), f)
+    P = gpu_solve(nx, ny, nz, bc, f, box=box)
+    zero_mode_column = bc[0:2] in ("PP", "NN") and bc[2:4] in ("PP", "NN")
+    assert O.rel_l2(P, Q) <= (1e-11 if zero_mode_column else TOL)
+    if bc[2:4] != "PP":
+        Qe = O.solve(O.problem(nx, ny, nz, bc, box=box, compat_zero_mode=0), f)
+        R = gpu_solve(nx, ny, nz, bc, f, box=box, precision=1, max_sweeps=3, compat_zero_mode=0)
+        assert O.rel_l2(R.real, Qe.real) <= 1e-10
+
+
 def test_x_periodic_y_cosine_reproduces_reference_quirk():
     z = np.load(os.path.join(os.path.dirname(__file__), "golden", "pp_nn_dd_quirk.npz"))
     P = gpu_solve(8, 8, 8, "PPNNDD", z["f_re"])
@@ -184,5 +211,10 @@ def test_errors_are_returned_not_fatal():
         with pytest.raises(pp.PittPackError):
             M.pittPack()  # no RHS yet
     with pytest.raises(pp.PittPackError) as e:
-        pp.make_Poisson(8, 8, 4097)  # z systems longer than the z solve's 4096 rows
+        pp.make_Poisson(4, 4, 30000)  # z systems longer than one CTA's shared memory holds
     assert e.value.code == 27
+    with pp.make_Poisson(4, 4, 20000) as M:
+        M.assignBoundary("NNNNDD")  # real spectra: a 20000-row column fits
+        with pytest.raises(pp.PittPackError) as e:
+            M.assignBoundary("PPPPDD")  # complex spectra: twice the bytes, it does not
+        assert e.value.code == 27
