@@ -70,6 +70,25 @@ struct PPLinePassArgs {
 // shared memory of the generic kernel: two buffers of L lines of nfft complex
 // points in FP64, or in FP32 (fp32)
 size_t pp_line_pass_smem(int L, int nfft, bool fp32 = false);
+
+// Lines whose FFT length nf is past one generic-kernel tile (pp_longline.cu):
+// the FFT in four steps, nf = n1 n2, through a global scratch array of
+// nplanes x nlines x nf complex points
+struct PPLongPlan {
+    int n1, n2;
+    PPFftPlan f1, f2;      // plans of n1 and n2 with their FP64 twiddles
+    const void* tw1f;      // FP32 twiddles of n1 and n2
+    const void* tw2f;
+    const double2* twl;    // W_nf^j, j < nf, FP64 and FP32
+    const void* twlf;
+    void* scratch;
+};
+// the split nf = n1 n2 (n1 <= n2, nearest the square root, both within one
+// generic-kernel tile); false where there is none (a prime beyond that size)
+bool pp_long_split(int nf, int* n1, int* n2);
+size_t pp_long_scratch_bytes(long lines, int nf);
+cudaError_t pp_launch_long_line_pass(const PPLinePassArgs& a, const PPLongPlan& lp, bool inverse, bool strided,
+                                     bool in_cplx, bool out_cplx, cudaStream_t st, bool fp32);
 // power-of-two lengths 16..2048: complex FFT lines per CTA (0 = not covered);
 // a tile holds this many data lines for the periodic family and twice as many
 // for the real families

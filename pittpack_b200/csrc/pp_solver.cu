@@ -66,7 +66,37 @@ struct DirTables {
     DevBuf eig;  // -2 + 2 cos((k + num) f / (n + den)), k < n
     DevBuf twf;  // FP32 copies for the refined mixed-precision solve
     DevBuf csf;
+    // lines past one tile of the generic kernel: the four-step split of
+    // fft.n (n1 = 0: not used), its plans and twiddles, the handle's scratch
+    int n1 = 0, n2 = 0;
+    PPFftPlan f1{}, f2{};
+    DevBuf tw1, tw2, tw1f, tw2f;
+    void* scratch = nullptr;
+    void free_all()
+    {
+        tw.free(); cs.free(); eig.free(); twf.free(); csf.free();
+        tw1.free(); tw2.free(); tw1f.free(); tw2f.free();
+    }
 };
+
+// FFT twiddles W_n^m, m < n, in long double rounded to FP64 and FP32
+cudaError_t upload_twiddles(int n, DevBuf& t64, DevBuf& t32)
+{
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    std::vector<double2> tw(n);
+    std::vector<float2> twf(n);
+    for (int m = 0; m < n; ++m) {
+        const long double a = -two_pi * (long double)m / (long double)n;
+        tw[m] = make_double2((double)cosl(a), (double)sinl(a));
+        twf[m] = make_float2((float)tw[m].x, (float)tw[m].y);
+    }
+    cudaError_t e;
+    if ((e = t64.alloc(sizeof(double2) * n)) != cudaSuccess || (e = t32.alloc(sizeof(float2) * n)) != cudaSuccess ||
+        (e = cudaMemcpy(t64.p, tw.data(), sizeof(double2) * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(t32.p, twf.data(), sizeof(float2) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return e;
+    return cudaSuccess;
+}
 
 }  // namespace
 
@@ -91,6 +121,7 @@ struct pp_solver_s {
     DevBuf zero1;  // one double 0.0 (eigen table of the zero-mode system)
     DevBuf mgstats;  // multigrid z solve: max cycles, unconverged systems (2 ints)
     DevBuf zmean;    // zero-mean option: partial sums and the mean
+    DevBuf wlong;    // four-step scratch of the directions past one generic-kernel tile
     int last_sweeps = 0;
     DevBuf lift[6];
     PPLift liftv{};
@@ -129,9 +160,21 @@ int build_dir(pp_solver_s* h, DirTables& t, int n, int kind)
     std::vector<int> r;
     if (!radix_plan(nf, r)) return PP_UNSUPPORTED;
     // the generic kernel holds a tile of at least one line (two buffers) in
-    // shared memory: lengths past that limit, outside the register kernels,
-    // are not taken
-    if (pp_lp2_lpc(n) == 0 && pp_lpm_lpc(n) == 0 && pp_line_pass_smem(1, nf) > 227 * 1024) return PP_UNSUPPORTED;
+    // shared memory: longer lines, outside the register kernels, run the
+    // four-step FFT through global memory (pp_longline.cu) where nf splits
+    t.n1 = t.n2 = 0;
+    if (pp_lp2_lpc(n) == 0 && pp_lpm_lpc(n) == 0 && pp_line_pass_smem(1, nf) > 227 * 1024) {
+        int n1 = 0, n2 = 0;
+        if (!pp_long_split(nf, &n1, &n2) || !pp_fft_plan(n1, &t.f1) || !pp_fft_plan(n2, &t.f2)) return PP_UNSUPPORTED;
+        cudaError_t e;
+        if ((e = upload_twiddles(n1, t.tw1, t.tw1f)) != cudaSuccess ||
+            (e = upload_twiddles(n2, t.tw2, t.tw2f)) != cudaSuccess)
+            return set_cuda_error(h, e, e == cudaErrorMemoryAllocation ? PP_ALLOCATION_FAIL : PP_CUDA_ERROR);
+        t.f1.tw = t.tw1.as<double2>();
+        t.f2.tw = t.tw2.as<double2>();
+        t.n1 = n1;
+        t.n2 = n2;
+    }
     t.fft.n = nf;
     t.fft.npass = (int)r.size();
     for (size_t i = 0; i < r.size(); ++i) t.fft.radix[i] = r[i];
@@ -380,6 +423,20 @@ cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool s
     int lpc = pp_lp2_lpc(d.n);
     const bool mixed = lpc == 0 && pp_lpm_lpc(d.n) > 0;
     if (mixed) lpc = pp_lpm_lpc(d.n);
+    if (d.n1 > 0) {
+        PPLongPlan lp{};
+        lp.n1 = d.n1;
+        lp.n2 = d.n2;
+        lp.f1 = d.f1;
+        lp.f2 = d.f2;
+        lp.tw1f = d.tw1f.p;
+        lp.tw2f = d.tw2f.p;
+        lp.twl = d.tw.as<double2>();
+        lp.twlf = d.twf.p;
+        lp.scratch = d.scratch;
+        a.cs2 = d.csf.p;
+        return pp_launch_long_line_pass(a, lp, inverse, strided, in_cplx, out_cplx, st, fp32);
+    }
     if (fp32 && lpc == 0) {
         a.fft = d.fft;
         a.tw = d.twf.p;
@@ -513,8 +570,28 @@ int zero_mean(pp_solver_s* h)
     return e == cudaSuccess ? PP_SUCCESS : set_cuda_error(h, e, PP_CUDA_ERROR);
 }
 
+// the four-step scratch of the long directions, sized for the larger pass
+// (x: ny x nz lines, y: spectrum columns x nz lines, of fft.n points)
+int ensure_long_scratch(pp_solver_s* h)
+{
+    if (h->tx.n1 == 0 && h->ty.n1 == 0) return PP_SUCCESS;
+    const int hc = half_spectrum_cols(h);
+    const long ncol = hc ? hc : h->nx;
+    size_t need = 0;
+    if (h->tx.n1) need = std::max(need, pp_long_scratch_bytes((long)h->ny * h->nz, h->tx.fft.n));
+    if (h->ty.n1) need = std::max(need, pp_long_scratch_bytes(ncol * h->nz, h->ty.fft.n));
+    if (h->wlong.bytes < need) {
+        const cudaError_t e = h->wlong.alloc(need);
+        if (e != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+    }
+    h->tx.scratch = h->wlong.p;
+    h->ty.scratch = h->wlong.p;
+    return PP_SUCCESS;
+}
+
 int launch_solve(pp_solver_s* h)
 {
+    if (const int rc = ensure_long_scratch(h)) return rc;
     const int nx = h->nx, ny = h->ny, nz = h->nz;
     const int kx = h->tx.kind, ky = h->ty.kind;
     const bool x_cplx = kx == PP_KIND_FFT;  // after the x transform
@@ -668,6 +745,7 @@ bool has_zero_mode(int kx, int ky)
 // half of B.
 int launch_mixed(pp_solver_s* h)
 {
+    if (const int rc = ensure_long_scratch(h)) return rc;
     const int nx = h->nx, ny = h->ny, nz = h->nz;
     const int kx = h->tx.kind, ky = h->ty.kind;
     const bool x_cplx = kx == PP_KIND_FFT;
@@ -950,9 +1028,9 @@ int pp_destroy(pp_handle h)
     h->zero1.free();
     h->mgstats.free();
     h->zmean.free();
-    h->tx.twf.free(); h->tx.csf.free(); h->ty.twf.free(); h->ty.csf.free();
-    h->tx.tw.free(); h->tx.cs.free(); h->tx.eig.free();
-    h->ty.tw.free(); h->ty.cs.free(); h->ty.eig.free();
+    h->wlong.free();
+    h->tx.free_all();
+    h->ty.free_all();
     delete h;
     return PP_SUCCESS;
 }
@@ -1389,6 +1467,9 @@ int pp_workspace_bytes(pp_handle h, size_t* bytes)
     for (const DirTables* t : {&h->tx, &h->ty})
         b += t->tw.bytes + t->cs.bytes + t->eig.bytes + t->twf.bytes + t->csf.bytes;
     b += h->psum.bytes + h->part.bytes + h->errc.bytes + h->zero1.bytes + h->mgstats.bytes + h->zmean.bytes;
+    b += h->wlong.bytes;
+    for (const DirTables* t : {&h->tx, &h->ty})
+        b += t->tw1.bytes + t->tw2.bytes + t->tw1f.bytes + t->tw2f.bytes;
     *bytes = b;
     return PP_SUCCESS;
 }
