@@ -73,19 +73,33 @@ size_t pp_line_pass_smem(int L, int nfft, bool fp32 = false);
 
 // Lines whose FFT length nf is past one generic-kernel tile (pp_longline.cu):
 // the FFT in four steps, nf = n1 n2, through a global scratch array of
-// nplanes x nlines x nf complex points
+// nplanes x nlines x nf complex points; or, where nf has a prime factor past
+// one tile, by the chirp z-transform: a cyclic convolution of length
+// M = n1 n2 (a power of two >= 2 nf - 1) by two four-step FFTs
 struct PPLongPlan {
     int n1, n2;
     PPFftPlan f1, f2;      // plans of n1 and n2 with their FP64 twiddles
     const void* tw1f;      // FP32 twiddles of n1 and n2
     const void* tw2f;
-    const double2* twl;    // W_nf^j, j < nf, FP64 and FP32
+    const double2* twl;    // W_(n1 n2)^j, j < n1 n2, FP64 and FP32
     const void* twlf;
     void* scratch;
+    // chirp z-transform (M = n1 n2 > 0): c_k = e^{i pi k^2 / nf}, k < nf, and
+    // the FFT of the chirp kernel for the forward and backward transforms, in
+    // the four-step output order; FP64 and FP32
+    int M;
+    int nf;                // the transform's FFT length (n1 n2 without the chirp z-transform)
+    const double2* chirp;
+    const void* chirpf;
+    const double2* bhat[2];
+    const void* bhatf[2];
 };
 // the split nf = n1 n2 (n1 <= n2, nearest the square root, both within one
 // generic-kernel tile); false where there is none (a prime beyond that size)
 bool pp_long_split(int nf, int* n1, int* n2);
+// the chirp z-transform's convolution length for nf (a power of two >= 2 nf - 1)
+// and its split; false past the four-step's reach
+bool pp_bluestein_split(int nf, int* M, int* n1, int* n2);
 size_t pp_long_scratch_bytes(long lines, int nf);
 cudaError_t pp_launch_long_line_pass(const PPLinePassArgs& a, const PPLongPlan& lp, bool inverse, bool strided,
                                      bool in_cplx, bool out_cplx, cudaStream_t st, bool fp32);

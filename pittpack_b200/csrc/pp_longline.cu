@@ -1,8 +1,8 @@
 // Transform passes for lines longer than one tile of the generic kernel holds
 // (its two shared-memory buffers of one line: an FFT length past 7264 in
 // FP64).  The reference hands any length to cuFFT / FFTW
-// (src/poissonGPU.cpp:13, src/poissonCPU.cpp:56); here such a pass runs in
-// four steps through a global scratch array W:
+// (src/poissonGPU.cpp:13, src/poissonCPU.cpp:56); here such a pass runs
+// through a global scratch array W:
 //
 //   pre      the family's load and pre-processing of the generic kernel
 //            (pp_linepass.cu, steps 1-2), one FFT input point per thread,
@@ -14,6 +14,17 @@
 //            at k1 n2 + k2;
 //   post     the family's post-processing and store of the generic kernel
 //            (step 4), reading X through that index map.
+//
+// An FFT length with a prime factor past one tile takes the chirp
+// z-transform (Bluestein): with c_k = e^{i pi k^2 / nf},
+//   sum_m V_m e^{-2 pi i m k / nf} = conj(c_k) sum_m (V_m conj(c_m)) c_{k-m},
+// a cyclic convolution of length M (a power of two >= 2 nf - 1, split
+// M = n1 n2): the pre kernel writes V conj(c) padded with zeros to M points,
+// a four-step FFT leaves its spectrum in the transposed order, which is
+// multiplied by the chirp kernel's spectrum (a table in that order), and the
+// inverse four-step run in the reverse order of its steps returns the
+// convolution in natural order; the post kernel reads conj(c_k) / M times it.
+// The backward transform conjugates every chirp.
 //
 // W keeps a line's points contiguous for the contiguous (x) passes and the
 // lines of a plane contiguous ([plane][m][line]) for the strided (y) passes,
@@ -74,15 +85,27 @@ PP_D typename LlVec<R>::type ll_load(const PPLinePassArgs& a, const R* src, bool
     return v;
 }
 
-// position of point m of line (p, l) in W
-PP_D long ll_w(bool strided, int nl, int nf, int p, int l, int m)
+// position of point m of line (p, l) in W (lines of lw points)
+PP_D long ll_w(bool strided, int nl, int lw, int p, int l, int m)
 {
-    return strided ? ((long)p * nf + m) * nl + l : ((long)p * nl + l) * nf + m;
+    return strided ? ((long)p * lw + m) * nl + l : ((long)p * nl + l) * lw + m;
+}
+
+// the chirp factor of point k: conj(c_k) forward, c_k backward
+template <typename C>
+PP_D C ll_chirp(const C* chirp, int k, int back)
+{
+    C c = __ldg(&chirp[k]);
+    if (!back) c.y = -c.y;
+    return c;
 }
 
 // ---- pre: one FFT input point per thread ------------------------------------------------
+// lw = nf (four-step), or M (chirp z-transform: the input times the chirp
+// factor, zero from nf to M)
 template <typename R>
-__global__ void ll_pre_kernel(PPLinePassArgs a, typename LlVec<R>::type* W, int nf, int inverse, int strided,
+__global__ void ll_pre_kernel(PPLinePassArgs a, typename LlVec<R>::type* W, int nf, int lw,
+                              const typename LlVec<R>::type* __restrict__ chirp, int back, int inverse, int strided,
                               int in_cplx)
 {
     using C = typename LlVec<R>::type;
@@ -92,19 +115,23 @@ __global__ void ll_pre_kernel(PPLinePassArgs a, typename LlVec<R>::type* W, int 
     const bool quarter = pp_kind_is_quarter(kind);
     const bool q_odd = quarter && (n & 1);
     const bool staged = quarter || (inverse && kind != PP_KIND_FFT);
-    const long total = (long)a.nplanes * nl * nf;
+    const long total = (long)a.nplanes * nl * lw;
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
         int p, l, k;
         if (strided) {
-            p = (int)(idx / ((long)nf * nl));
-            const long r = idx - (long)p * nf * nl;
+            p = (int)(idx / ((long)lw * nl));
+            const long r = idx - (long)p * lw * nl;
             k = (int)(r / nl);
             l = (int)(r - (long)k * nl);
         } else {
-            const long g = idx / nf;
-            k = (int)(idx - g * nf);
+            const long g = idx / lw;
+            k = (int)(idx - g * lw);
             p = (int)(g / nl);
             l = (int)(g - (long)p * nl);
+        }
+        if (k >= nf) {
+            W[ll_w(strided, nl, lw, p, l, k)] = mkc<C>((R)0, (R)0);
+            continue;
         }
         const long base = (long)p * a.plane_stride + (long)l * a.line_stride;
         // the real line the staged families transform (reversed / sign-swapped)
@@ -154,7 +181,19 @@ __global__ void ll_pre_kernel(PPLinePassArgs a, typename LlVec<R>::type* W, int 
             V.y = -((R)0.5 * (t.y * xk - t.x * xn));
             V.x = (R)0.5 * (t.x * xk + t.y * xn);
         }
-        W[ll_w(strided, nl, nf, p, l, k)] = V;
+        if (chirp) V = c_mul(V, ll_chirp(chirp, k, back));
+        W[ll_w(strided, nl, lw, p, l, k)] = V;
+    }
+}
+
+// ---- chirp z-transform: the spectrum times the chirp kernel's (same order) ---------
+template <typename R>
+__global__ void ll_kernel_mul(typename LlVec<R>::type* W, const typename LlVec<R>::type* __restrict__ bhat, long total,
+                              int nl, int lw, int strided)
+{
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+        const int m = strided ? (int)((idx / nl) % lw) : (int)(idx % lw);
+        W[idx] = c_mul(W[idx], __ldg(&bhat[m]));
     }
 }
 
@@ -176,13 +215,18 @@ __global__ void ll_twiddle_kernel(typename LlVec<R>::type* W, const typename LlV
 }
 
 // ---- post: one output element per thread -------------------------------------------------
+// nf: the transform's FFT length; M > 0: the chirp z-transform's convolution
+// length (X natural, times the chirp factor / M), else X at the four-step order
 template <typename R>
-__global__ void ll_post_kernel(PPLinePassArgs a, const typename LlVec<R>::type* W, int n1, int n2, int inverse,
-                               int strided, int out_cplx)
+__global__ void ll_post_kernel(PPLinePassArgs a, const typename LlVec<R>::type* W, int nf, int n1, int n2, int M,
+                               const typename LlVec<R>::type* __restrict__ chirp, int back, int inverse, int strided,
+                               int out_cplx)
 {
     using C = typename LlVec<R>::type;
     const C* cs = sizeof(R) == 8 ? reinterpret_cast<const C*>(a.cs) : reinterpret_cast<const C*>(a.cs2);
-    const int n = a.n, kind = a.kind, nl = a.nlines, nf = n1 * n2;
+    const int n = a.n, kind = a.kind, nl = a.nlines;
+    const int lw = M ? M : nf;
+    const R inv_m = M ? (R)1 / (R)M : (R)1;
     const bool quarter = pp_kind_is_quarter(kind);
     const bool q_odd = quarter && (n & 1);
     const long total = (long)a.nplanes * nl * n;
@@ -199,10 +243,12 @@ __global__ void ll_post_kernel(PPLinePassArgs a, const typename LlVec<R>::type* 
             p = (int)(g / nl);
             l = (int)(g - (long)p * nl);
         }
-        // X[k] of this line: the four-step leaves it at (k mod n1) n2 + k / n1
+        // X[k] of this line: the four-step leaves it at (k mod n1) n2 + k / n1;
+        // the chirp z-transform's convolution at k, times the chirp factor / M
         auto Xk = [&](int k) -> C {
+            if (M) return c_scale(c_mul(W[ll_w(strided, nl, lw, p, l, k)], ll_chirp(chirp, k, back)), inv_m);
             const int k2 = k / n1;
-            return W[ll_w(strided, nl, nf, p, l, (k - k2 * n1) * n2 + k2)];
+            return W[ll_w(strided, nl, lw, p, l, (k - k2 * n1) * n2 + k2)];
         };
         C o;
         if (kind == PP_KIND_FFT) {
@@ -282,69 +328,96 @@ int ll_lines(int n, bool fp32)
     return L;
 }
 
+// one four-step step on the generic kernel, in place over W (lines of lw =
+// n1 n2 points): A, the n1-point FFTs over the stride-n2 columns; B, the
+// n2-point FFTs over the contiguous rows
+cudaError_t ll_step(void* W, const PPLongPlan& lp, bool step_a, int nl, int nplanes, bool strided, bool backward,
+                    bool fp32, const PPLinePassArgs& a, cudaStream_t st)
+{
+    const int n1 = lp.n1, n2 = lp.n2, lw = n1 * n2;
+    PPLinePassArgs s{};
+    s.src = static_cast<const double*>(W);
+    s.dst = static_cast<double*>(W);
+    s.kind = PP_KIND_FFT;
+    s.out_scale = 1.0;
+    s.nx = a.nx;
+    s.ny = a.ny;
+    s.nz = a.nz;
+    if (step_a) {
+        s.n = n1;
+        s.fft = lp.f1;
+        s.tw = lp.tw1f;
+        s.elem_stride = strided ? (long)n2 * nl : n2;
+        s.line_stride = 1;
+        s.nlines = strided ? n2 * nl : n2;
+        s.nplanes = strided ? nplanes : nplanes * nl;
+        s.plane_stride = strided ? (long)lw * nl : lw;
+    } else {
+        s.n = n2;
+        s.fft = lp.f2;
+        s.tw = lp.tw2f;
+        s.elem_stride = strided ? nl : 1;
+        s.line_stride = strided ? 1 : n2;
+        s.nlines = strided ? nl : n1;
+        s.nplanes = strided ? nplanes * n1 : nplanes * nl;
+        s.plane_stride = strided ? (long)n2 * nl : lw;
+    }
+    s.L = ll_lines(s.n, fp32);
+    s.tiles_per_plane = (s.nlines + s.L - 1) / s.L;
+    // step A reads lines at a stride (adjacent lines adjacent in memory);
+    // step B is contiguous in the line layout, strided in the plane layout
+    return pp_launch_line_pass(s, backward, step_a ? true : strided, true, true, st, fp32);
+}
+
 template <typename R>
 cudaError_t ll_launch(const PPLinePassArgs& a, const PPLongPlan& lp, bool inverse, bool strided, bool in_cplx,
                       bool out_cplx, cudaStream_t st)
 {
     using C = typename LlVec<R>::type;
     const bool fp32 = sizeof(R) == 4;
-    const int n1 = lp.n1, n2 = lp.n2, nf = n1 * n2, nl = a.nlines;
+    const int n1 = lp.n1, n2 = lp.n2, lw = n1 * n2, nl = a.nlines;
+    const int nf = lp.M ? lp.nf : lw;
     const bool backward = inverse && !pp_kind_is_quarter(a.kind);
+    const int back = backward ? 1 : 0;
     C* W = static_cast<C*>(lp.scratch);
-    const long total = (long)a.nplanes * nl * nf;
-    ll_pre_kernel<R><<<ll_blocks(total), 256, 0, st>>>(a, W, nf, inverse, strided, in_cplx);
+    const C* chirp = lp.M ? static_cast<const C*>(fp32 ? lp.chirpf : (const void*)lp.chirp) : nullptr;
+    const C* twl = static_cast<const C*>(fp32 ? lp.twlf : (const void*)lp.twl);
+    const long total = (long)a.nplanes * nl * lw;
+    ll_pre_kernel<R><<<ll_blocks(total), 256, 0, st>>>(a, W, nf, lw, chirp, back, inverse, strided, in_cplx);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    // the two FFT steps on the generic kernel, in place
-    PPLinePassArgs s{};
-    s.src = reinterpret_cast<const double*>(W);
-    s.dst = reinterpret_cast<double*>(W);
-    s.kind = PP_KIND_FFT;
-    s.out_scale = 1.0;
-    s.nx = a.nx;
-    s.ny = a.ny;
-    s.nz = a.nz;
-    // step 1: n1 points at stride n2 (x n_l in the strided layout)
-    s.n = n1;
-    s.fft = lp.f1;
-    s.tw = lp.tw1f;
-    s.L = ll_lines(n1, fp32);
-    s.elem_stride = strided ? (long)n2 * nl : n2;
-    s.line_stride = 1;
-    s.nlines = strided ? n2 * nl : n2;
-    s.nplanes = strided ? a.nplanes : a.nplanes * nl;
-    s.plane_stride = strided ? (long)nf * nl : nf;
-    s.tiles_per_plane = (s.nlines + s.L - 1) / s.L;
-    if ((e = pp_launch_line_pass(s, backward, true, true, true, st, fp32)) != cudaSuccess) return e;
-    ll_twiddle_kernel<R><<<ll_blocks(total), 256, 0, st>>>(W, static_cast<const C*>(fp32 ? lp.twlf : (const void*)lp.twl),
-                                                          total, nl, nf, n2, strided, backward);
+    // forward four-step (the transform's own sign, or -1 for the convolution)
+    const bool fsign = lp.M ? false : backward;
+    if ((e = ll_step(W, lp, true, nl, a.nplanes, strided, fsign, fp32, a, st)) != cudaSuccess) return e;
+    ll_twiddle_kernel<R><<<ll_blocks(total), 256, 0, st>>>(W, twl, total, nl, lw, n2, strided, fsign);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    // step 2: n2 contiguous points (stride n_l in the strided layout)
-    s.n = n2;
-    s.fft = lp.f2;
-    s.tw = lp.tw2f;
-    s.L = ll_lines(n2, fp32);
-    if (strided) {
-        s.elem_stride = nl;
-        s.line_stride = 1;
-        s.nlines = nl;
-        s.nplanes = a.nplanes * n1;
-        s.plane_stride = (long)n2 * nl;
-    } else {
-        s.elem_stride = 1;
-        s.line_stride = n2;
-        s.nlines = n1;
-        s.nplanes = a.nplanes * nl;
-        s.plane_stride = nf;
+    if ((e = ll_step(W, lp, false, nl, a.nplanes, strided, fsign, fp32, a, st)) != cudaSuccess) return e;
+    if (lp.M) {
+        // times the chirp kernel's spectrum, then the inverse four-step in
+        // the reverse order of its steps (transposed in, natural out)
+        const C* bhat = static_cast<const C*>(fp32 ? lp.bhatf[back] : (const void*)lp.bhat[back]);
+        ll_kernel_mul<R><<<ll_blocks(total), 256, 0, st>>>(W, bhat, total, nl, lw, strided);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = ll_step(W, lp, false, nl, a.nplanes, strided, true, fp32, a, st)) != cudaSuccess) return e;
+        ll_twiddle_kernel<R><<<ll_blocks(total), 256, 0, st>>>(W, twl, total, nl, lw, n2, strided, 1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = ll_step(W, lp, true, nl, a.nplanes, strided, true, fp32, a, st)) != cudaSuccess) return e;
     }
-    s.tiles_per_plane = (s.nlines + s.L - 1) / s.L;
-    if ((e = pp_launch_line_pass(s, backward, strided, true, true, st, fp32)) != cudaSuccess) return e;
     const long outs = (long)a.nplanes * nl * a.n;
-    ll_post_kernel<R><<<ll_blocks(outs), 256, 0, st>>>(a, W, n1, n2, inverse, strided, out_cplx);
+    ll_post_kernel<R><<<ll_blocks(outs), 256, 0, st>>>(a, W, nf, n1, n2, lp.M, chirp, back, inverse, strided, out_cplx);
     return cudaGetLastError();
 }
 
 }  // namespace
+
+bool pp_bluestein_split(int nf, int* M, int* n1, int* n2)
+{
+    long m = 1;
+    while (m < 2L * nf - 1) m <<= 1;
+    if (m > (1L << 26)) return false;
+    *M = (int)m;
+    return pp_long_split((int)m, n1, n2);
+}
 
 bool pp_long_split(int nf, int* n1, int* n2)
 {

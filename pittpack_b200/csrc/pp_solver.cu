@@ -72,12 +72,109 @@ struct DirTables {
     PPFftPlan f1{}, f2{};
     DevBuf tw1, tw2, tw1f, tw2f;
     void* scratch = nullptr;
+    // fft.n with a prime factor past one tile: the chirp z-transform over
+    // M = n1 n2 points (M = 0: not used), W_M twiddles, chirp, kernel spectra
+    int M = 0;
+    DevBuf twm, twmf, chirp, chirpf, bhat[2], bhatf[2];
     void free_all()
     {
         tw.free(); cs.free(); eig.free(); twf.free(); csf.free();
         tw1.free(); tw2.free(); tw1f.free(); tw2f.free();
+        twm.free(); twmf.free(); chirp.free(); chirpf.free();
+        for (int b = 0; b < 2; ++b) {
+            bhat[b].free();
+            bhatf[b].free();
+        }
+    }
+    size_t long_bytes() const
+    {
+        size_t b = tw1.bytes + tw2.bytes + tw1f.bytes + tw2f.bytes + twm.bytes + twmf.bytes + chirp.bytes + chirpf.bytes;
+        for (int q = 0; q < 2; ++q) b += bhat[q].bytes + bhatf[q].bytes;
+        return b;
     }
 };
+
+// upload a table in FP64 and its FP32 rounding
+cudaError_t upload_pair(const std::vector<double2>& v, DevBuf& t64, DevBuf& t32)
+{
+    std::vector<float2> f(v.size());
+    for (size_t m = 0; m < v.size(); ++m) f[m] = make_float2((float)v[m].x, (float)v[m].y);
+    cudaError_t e;
+    if ((e = t64.alloc(sizeof(double2) * v.size())) != cudaSuccess ||
+        (e = t32.alloc(sizeof(float2) * v.size())) != cudaSuccess ||
+        (e = cudaMemcpy(t64.p, v.data(), sizeof(double2) * v.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(t32.p, f.data(), sizeof(float2) * v.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return e;
+    return cudaSuccess;
+}
+
+// in-place radix-2 FFT (sign -1) of a power-of-two length in long double
+void host_fft_pow2(std::vector<long double>& re, std::vector<long double>& im)
+{
+    const size_t n = re.size();
+    for (size_t i = 1, j = 0; i < n; ++i) {
+        size_t bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            std::swap(re[i], re[j]);
+            std::swap(im[i], im[j]);
+        }
+    }
+    const long double pi_l = 3.141592653589793238462643383279502884L;
+    for (size_t len = 2; len <= n; len <<= 1) {
+        const size_t h = len / 2;
+        for (size_t k = 0; k < h; ++k) {
+            const long double a = -2.0L * pi_l * (long double)k / (long double)len;
+            const long double wr = cosl(a), wi = sinl(a);
+            for (size_t s = 0; s < n; s += len) {
+                const size_t u = s + k, v = s + k + h;
+                const long double xr = re[v] * wr - im[v] * wi, xi = re[v] * wi + im[v] * wr;
+                re[v] = re[u] - xr;
+                im[v] = im[u] - xi;
+                re[u] += xr;
+                im[u] += xi;
+            }
+        }
+    }
+}
+
+// the chirp z-transform's tables for an FFT of nf points over M = n1 n2:
+// c_k = e^{i pi k^2 / nf} (k^2 reduced mod 2 nf), and the spectra of the
+// chirp kernel b (b_j = c_j, b_{M-j} = c_j for 0 < j < nf; conjugated for the
+// backward transform) in the four-step output order (k at (k mod n1) n2 + k / n1)
+cudaError_t build_chirp_tables(DirTables& t, int nf)
+{
+    const long double pi_l = 3.141592653589793238462643383279502884L;
+    const int M = t.M, n1 = t.n1, n2 = t.n2;
+    std::vector<long double> cr(nf), ci(nf);
+    std::vector<double2> c(nf);
+    for (int k = 0; k < nf; ++k) {
+        const long q = (long)((long long)k * k % (2LL * nf));
+        const long double a = pi_l * (long double)q / (long double)nf;
+        cr[k] = cosl(a);
+        ci[k] = sinl(a);
+        c[k] = make_double2((double)cr[k], (double)ci[k]);
+    }
+    cudaError_t e = upload_pair(c, t.chirp, t.chirpf);
+    for (int back = 0; back < 2 && e == cudaSuccess; ++back) {
+        std::vector<long double> re(M, 0.0L), im(M, 0.0L);
+        const long double s = back ? -1.0L : 1.0L;
+        for (int j = 0; j < nf; ++j) {
+            re[j] = cr[j];
+            im[j] = s * ci[j];
+            if (j > 0) {
+                re[M - j] = cr[j];
+                im[M - j] = s * ci[j];
+            }
+        }
+        host_fft_pow2(re, im);
+        std::vector<double2> b(M);
+        for (int k = 0; k < M; ++k) b[(size_t)(k % n1) * n2 + k / n1] = make_double2((double)re[k], (double)im[k]);
+        e = upload_pair(b, t.bhat[back], t.bhatf[back]);
+    }
+    return e;
+}
 
 // FFT twiddles W_n^m, m < n, in long double rounded to FP64 and FP32
 cudaError_t upload_twiddles(int n, DevBuf& t64, DevBuf& t32)
@@ -162,18 +259,25 @@ int build_dir(pp_solver_s* h, DirTables& t, int n, int kind)
     // the generic kernel holds a tile of at least one line (two buffers) in
     // shared memory: longer lines, outside the register kernels, run the
     // four-step FFT through global memory (pp_longline.cu) where nf splits
-    t.n1 = t.n2 = 0;
+    t.n1 = t.n2 = t.M = 0;
     if (pp_lp2_lpc(n) == 0 && pp_lpm_lpc(n) == 0 && pp_line_pass_smem(1, nf) > 227 * 1024) {
-        int n1 = 0, n2 = 0;
-        if (!pp_long_split(nf, &n1, &n2) || !pp_fft_plan(n1, &t.f1) || !pp_fft_plan(n2, &t.f2)) return PP_UNSUPPORTED;
-        cudaError_t e;
-        if ((e = upload_twiddles(n1, t.tw1, t.tw1f)) != cudaSuccess ||
-            (e = upload_twiddles(n2, t.tw2, t.tw2f)) != cudaSuccess)
-            return set_cuda_error(h, e, e == cudaErrorMemoryAllocation ? PP_ALLOCATION_FAIL : PP_CUDA_ERROR);
-        t.f1.tw = t.tw1.as<double2>();
-        t.f2.tw = t.tw2.as<double2>();
+        // four-step where nf splits into two tiles, else the chirp z-transform
+        int n1 = 0, n2 = 0, M = 0;
+        if (!pp_long_split(nf, &n1, &n2) && !pp_bluestein_split(nf, &M, &n1, &n2)) return PP_UNSUPPORTED;
+        if (!pp_fft_plan(n1, &t.f1) || !pp_fft_plan(n2, &t.f2)) return PP_UNSUPPORTED;
         t.n1 = n1;
         t.n2 = n2;
+        t.M = M;
+        cudaError_t e;
+        if ((e = upload_twiddles(n1, t.tw1, t.tw1f)) != cudaSuccess ||
+            (e = upload_twiddles(n2, t.tw2, t.tw2f)) != cudaSuccess ||
+            (M && (e = upload_twiddles(M, t.twm, t.twmf)) != cudaSuccess) ||
+            (M && (e = build_chirp_tables(t, nf)) != cudaSuccess)) {
+            t.n1 = t.n2 = t.M = 0;
+            return set_cuda_error(h, e, e == cudaErrorMemoryAllocation ? PP_ALLOCATION_FAIL : PP_CUDA_ERROR);
+        }
+        t.f1.tw = t.tw1.as<double2>();
+        t.f2.tw = t.tw2.as<double2>();
     }
     t.fft.n = nf;
     t.fft.npass = (int)r.size();
@@ -431,9 +535,17 @@ cudaError_t line_pass(PPLinePassArgs a, const DirTables& d, bool inverse, bool s
         lp.f2 = d.f2;
         lp.tw1f = d.tw1f.p;
         lp.tw2f = d.tw2f.p;
-        lp.twl = d.tw.as<double2>();
-        lp.twlf = d.twf.p;
+        lp.twl = d.M ? d.twm.as<double2>() : d.tw.as<double2>();
+        lp.twlf = d.M ? d.twmf.p : d.twf.p;
         lp.scratch = d.scratch;
+        lp.M = d.M;
+        lp.nf = d.fft.n;
+        lp.chirp = d.chirp.as<double2>();
+        lp.chirpf = d.chirpf.p;
+        for (int b = 0; b < 2; ++b) {
+            lp.bhat[b] = d.bhat[b].as<double2>();
+            lp.bhatf[b] = d.bhatf[b].p;
+        }
         a.cs2 = d.csf.p;
         return pp_launch_long_line_pass(a, lp, inverse, strided, in_cplx, out_cplx, st, fp32);
     }
@@ -578,8 +690,9 @@ int ensure_long_scratch(pp_solver_s* h)
     const int hc = half_spectrum_cols(h);
     const long ncol = hc ? hc : h->nx;
     size_t need = 0;
-    if (h->tx.n1) need = std::max(need, pp_long_scratch_bytes((long)h->ny * h->nz, h->tx.fft.n));
-    if (h->ty.n1) need = std::max(need, pp_long_scratch_bytes(ncol * h->nz, h->ty.fft.n));
+    // lines of fft.n points, or of the chirp z-transform's M
+    if (h->tx.n1) need = std::max(need, pp_long_scratch_bytes((long)h->ny * h->nz, h->tx.n1 * h->tx.n2));
+    if (h->ty.n1) need = std::max(need, pp_long_scratch_bytes(ncol * h->nz, h->ty.n1 * h->ty.n2));
     if (h->wlong.bytes < need) {
         const cudaError_t e = h->wlong.alloc(need);
         if (e != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
@@ -1468,8 +1581,7 @@ int pp_workspace_bytes(pp_handle h, size_t* bytes)
         b += t->tw.bytes + t->cs.bytes + t->eig.bytes + t->twf.bytes + t->csf.bytes;
     b += h->psum.bytes + h->part.bytes + h->errc.bytes + h->zero1.bytes + h->mgstats.bytes + h->zmean.bytes;
     b += h->wlong.bytes;
-    for (const DirTables* t : {&h->tx, &h->ty})
-        b += t->tw1.bytes + t->tw2.bytes + t->tw1f.bytes + t->tw2f.bytes;
+    for (const DirTables* t : {&h->tx, &h->ty}) b += t->long_bytes();
     *bytes = b;
     return PP_SUCCESS;
 }

@@ -108,6 +108,26 @@ def job(spec: dict):
     return spec, P
 
 
+def long_line_rhs(nx: int, ny: int, nz: int, bc: str):
+    """The long-line parity cases' RHS: N(0, 1) (seed nx ny), complex for a
+    periodic x direction; (real, imaginary or None)."""
+    rng = np.random.default_rng(nx * ny)
+    fr = rng.standard_normal((nz, ny, nx))
+    fi = rng.standard_normal((nz, ny, nx)) if bc[0] == "P" else None
+    return fr, fi
+
+
+def long_line_oracle(nx: int, ny: int, nz: int, bc: str, compat: int, cells: bool):
+    """The oracle's solution of a long-line case (unit box, or unit cells)."""
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+
+    fr, fi = long_line_rhs(nx, ny, nz, bc)
+    box = (0, nx, 0, ny, 0, nz) if cells else (0, 1, 0, 1, 0, 1)
+    return O.solve(O.problem(nx, ny, nz, bc, box=box, compat_zero_mode=compat), fr, fi)
+
+
 def workers_for(bytes_per_job: float, jobs: int) -> int:
     """Worker processes that fit the host's free memory (and cores)."""
     try:

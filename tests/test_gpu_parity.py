@@ -113,12 +113,39 @@ def test_long_z_systems_vs_oracle(nx, ny, nz, bc):
         assert O.rel_l2(R.real, Qe.real) <= 1e-10
 
 
-@pytest.mark.parametrize("nx,ny,nz,bc", [(8192, 4, 3, "PPPPDD"), (7500, 4, 3, "DDNNDD"), (3703, 4, 3, "NDDDDD"),
-                                         (4, 10000, 3, "NNNNDD"), (4, 9000, 3, "PPPPNN"), (6, 16000, 3, "DDDNDD")])
-def test_long_lines_vs_oracle(nx, ny, nz, bc):
+LONG_LINES = [(8192, 4, 3, "PPPPDD"), (7500, 4, 3, "DDNNDD"), (3703, 4, 3, "NDDDDD"), (4, 10000, 3, "NNNNDD"),
+              (4, 9000, 3, "PPPPNN"), (6, 16000, 3, "DDDNDD"),
+              # prime lengths past one tile: the chirp z-transform
+              (7283, 4, 3, "NNDDDD"), (7297, 3, 3, "PPPPDD"), (4, 7307, 3, "DDDDNN"), (3, 7309, 3, "NDNDDD")]
+
+
+@pytest.fixture(scope="module")
+def long_line_oracle():
+    """The oracle's solutions of the long-line cases, computed in spawned
+    workers while the GPU runs (a prime-length line is an O(n^2) DFT there)."""
+    import multiprocessing as mp
+
+    import ref_jobs as J
+
+    jobs = {}
+    for nx, ny, nz, bc in LONG_LINES:
+        jobs[(nx, ny, nz, bc, 1, False)] = None
+        if bc[0] != "P":
+            jobs[(nx, ny, nz, bc, 0, True)] = None
+    pool = mp.get_context("spawn").Pool(J.workers_for(1e8, len(jobs)))
+    res = {k: pool.apply_async(J.long_line_oracle, k[:4] + k[4:]) for k in jobs}
+    yield lambda *k: res[k].get(timeout=1800)
+    pool.close()
+    pool.join()
+
+
+@pytest.mark.parametrize("nx,ny,nz,bc", LONG_LINES)
+def test_long_lines_vs_oracle(long_line_oracle, nx, ny, nz, bc):
     """x or y lines whose FFT is longer than one tile of the generic kernel
     (8192 and 7500 points; 7406 for the odd quarter-wave line of 3703; 10000,
-    9000 and 8000 in y): the four-step FFT through global memory, against the
+    9000 and 8000 in y): the four-step FFT through global memory; prime
+    lengths 7283, 7297, 7307 and the odd quarter-wave 7309 (an FFT of 14618 =
+    2 x 7309): the chirp z-transform over 16384 / 32768 points; against the
     oracle in the plain FP64 solve and, for the real families, the refined
     solve against the exact-zero-mode oracle.  The plain solve on the unit
     box; the refined one on unit cells (a box of nx x ny x nz): on the unit
@@ -127,18 +154,16 @@ def test_long_lines_vs_oracle(nx, ny, nz, bc):
     stalls near 1e-9 whatever the transforms (and on unit cells the long
     periodic y direction's lowest modes are nearly singular with Neumann z,
     which amplifies any rounding difference of the plain solve alike)."""
-    rng = np.random.default_rng(nx * ny)
-    f = rng.standard_normal((nz, ny, nx))
-    if bc[0] == "P":
-        f = f + 1j * rng.standard_normal((nz, ny, nx))
-    fr, fi = (f.real.copy(), f.imag.copy()) if np.iscomplexobj(f) else (f, None)
-    Q = O.solve(O.problem(nx, ny, nz, bc), fr, fi)
-    assert O.rel_l2(gpu_solve(nx, ny, nz, bc, f), Q) <= TOL
+    import ref_jobs as J
+
+    fr, fi = J.long_line_rhs(nx, ny, nz, bc)
+    f = fr if fi is None else fr + 1j * fi
+    P = gpu_solve(nx, ny, nz, bc, f)
+    assert O.rel_l2(P, long_line_oracle(nx, ny, nz, bc, 1, False)) <= TOL
     if fi is None:
         box = (0, nx, 0, ny, 0, nz)
-        Qe = O.solve(O.problem(nx, ny, nz, bc, box=box, compat_zero_mode=0), fr)
         R = gpu_solve(nx, ny, nz, bc, fr, box=box, precision=1, max_sweeps=3, compat_zero_mode=0)
-        assert O.rel_l2(R.real, Qe.real) <= 1e-10
+        assert O.rel_l2(R.real, long_line_oracle(nx, ny, nz, bc, 0, True).real) <= 1e-10
 
 
 def test_x_periodic_y_cosine_reproduces_reference_quirk():
