@@ -176,6 +176,20 @@ cudaError_t build_chirp_tables(DirTables& t, int nf)
     return e;
 }
 
+// the smallest prime factor of an FFT length that the chirp z-transform takes
+constexpr int PP_CHIRP_MIN_PRIME = 73;
+
+int largest_prime_factor(int n)
+{
+    int q = 1;
+    for (int p = 2; (long)p * p <= n; ++p)
+        while (n % p == 0) {
+            q = p;
+            n /= p;
+        }
+    return n > 1 ? n : q;
+}
+
 // FFT twiddles W_n^m, m < n, in long double rounded to FP64 and FP32
 cudaError_t upload_twiddles(int n, DevBuf& t64, DevBuf& t32)
 {
@@ -260,10 +274,17 @@ int build_dir(pp_solver_s* h, DirTables& t, int n, int kind)
     // shared memory: longer lines, outside the register kernels, run the
     // four-step FFT through global memory (pp_longline.cu) where nf splits
     t.n1 = t.n2 = t.M = 0;
-    if (pp_lp2_lpc(n) == 0 && pp_lpm_lpc(n) == 0 && pp_line_pass_smem(1, nf) > 227 * 1024) {
+    // lines past one generic-kernel tile, and lengths whose largest prime
+    // factor p makes the generic kernel's direct p-point pass (p^2 work per
+    // butterfly) slower than the chirp z-transform: measured on 64 x 64
+    // planes, p = 67 0.34 ms generic / 0.39 ms chirp per solve, p = 131
+    // 2.28 / 0.62, p = 1031 937 / 3.6, p = 4099 29500 / 14.4
+    const bool long_line = pp_line_pass_smem(1, nf) > 227 * 1024;
+    const bool big_prime = largest_prime_factor(nf) >= PP_CHIRP_MIN_PRIME;
+    if (pp_lp2_lpc(n) == 0 && pp_lpm_lpc(n) == 0 && (long_line || big_prime)) {
         // four-step where nf splits into two tiles, else the chirp z-transform
         int n1 = 0, n2 = 0, M = 0;
-        if (!pp_long_split(nf, &n1, &n2) && !pp_bluestein_split(nf, &M, &n1, &n2)) return PP_UNSUPPORTED;
+        if ((big_prime || !pp_long_split(nf, &n1, &n2)) && !pp_bluestein_split(nf, &M, &n1, &n2)) return PP_UNSUPPORTED;
         if (!pp_fft_plan(n1, &t.f1) || !pp_fft_plan(n2, &t.f2)) return PP_UNSUPPORTED;
         t.n1 = n1;
         t.n2 = n2;

@@ -37,7 +37,9 @@ CASES = ["PPPPDD", "NNNNDD", "NDNDDD", "DDDDDD", "NNDDNN", "DNPPND", "PPPPPP", "
 @pytest.mark.parametrize("shape", [(32, 64, 24), (64, 16, 7), (48, 40, 30), (24, 20, 18), (60, 36, 9), (32, 30, 16),
                                    # the residual kernel's edge cases: fewer rows than its 8-row tile,
                                    # odd nx (8-byte copies), partial x / y tiles, nz below its z chunk
-                                   (16, 4, 10), (45, 12, 10), (96, 100, 40), (128, 12, 3)])
+                                   (16, 4, 10), (45, 12, 10), (96, 100, 40), (128, 12, 3),
+                                   # prime lengths past 72: the chirp z-transform in FP32, x and y
+                                   (131, 24, 10), (24, 131, 10)])
 def test_refined_vs_exact_oracle(bc, shape):
     nx, ny, nz = shape
     if bc[0:2] == "PP" and bc[2:4] != "PP":
