@@ -49,8 +49,16 @@ enum { PP_PRECISION_FP64 = 0, PP_PRECISION_MIXED = 1 };
 /* z solver of the plain FP64 solve: the direct partition-method / PCR solve
  * (default; the reference's Thomas path, src/pencilDcmp.cpp:5066-5105), or
  * multigrid V-cycles on the same systems (the reference's alternate
- * MultiGrid solver, src/multiGrid.cpp:1105-1515) */
-enum { PP_ZSOLVE_DIRECT = 0, PP_ZSOLVE_MULTIGRID = 1 };
+ * MultiGrid solver, src/multiGrid.cpp:1105-1515), or one of two parity modes
+ * that reproduce the reference's alternates as its CPU build computes them
+ * (SOLUTIONMETHOD 1 and 2, src/pencilDcmp.cpp:6102-6148): its normalised PCR
+ * (src/pencilDcmp.cpp:5239-5270, src/triDiag.cpp:1442-1542; Dirichlet or
+ * Neumann z ends, nz <= 256 and not a power of two; its result is constant
+ * along z) and its CR-P (src/pencilDcmp.cpp:5275-5315,
+ * src/triDiag.cpp:1285-1437; Dirichlet z ends, nz = 2^L - 1).  Other sizes
+ * return PP_UNSUPPORTED from the solve.  Neither alternate solves the
+ * reference's own system: they exist to reproduce its outputs. */
+enum { PP_ZSOLVE_DIRECT = 0, PP_ZSOLVE_MULTIGRID = 1, PP_ZSOLVE_REF_PCR = 2, PP_ZSOLVE_REF_CRP = 3 };
 
 typedef struct pp_solver_s* pp_handle;
 
@@ -75,7 +83,8 @@ typedef struct {
     double tolerance;     /* target the caller checks; sweeps are a fixed count (no host sync) */
     int compat_zero_mode; /* 1 (default): reference zero-mode row replacement, src/triDiag.cpp:1753-1776 */
     int dirichlet_lift;   /* 1 (default): reference modifyRhsDirichlet, src/pencilDcmp.cpp:4623-4835 */
-    int z_solver;         /* PP_ZSOLVE_DIRECT (default) or PP_ZSOLVE_MULTIGRID (plain FP64 solve only) */
+    int z_solver;         /* PP_ZSOLVE_DIRECT (default), PP_ZSOLVE_MULTIGRID, PP_ZSOLVE_REF_PCR or
+                             PP_ZSOLVE_REF_CRP (the last three: plain FP64 solve only) */
     int zero_mean;        /* 0 (default) or 1: subtract the mean of the solution's real part, the
                              reference's ZERO_MEAN (subtractMeanValue, src/pencilDcmp.cpp:5649-5683) */
 } pp_options;

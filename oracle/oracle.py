@@ -36,6 +36,7 @@ class Problem(ctypes.Structure):
         ("dirichlet_lift", ctypes.c_int),
         ("face", ctypes.c_void_p * 6),
         ("zero_mean", ctypes.c_int),
+        ("z_method", ctypes.c_int),
     ]
 
 
@@ -77,7 +78,7 @@ def _dp(a):
 
 
 def problem(nx, ny, nz, bc, box=(0, 1, 0, 1, 0, 1), compat_zero_mode=1, dirichlet_lift=1, faces=None,
-            zero_mean=0) -> Problem:
+            zero_mean=0, z_method=0) -> Problem:
     """faces: {face 0..5: array} of boundary data (Dirichlet values / Neumann
     outward derivatives, shaped (nz, ny), (nz, nx) or (ny, nx) for x, y, z
     faces); zero_mean: subtract the solution's mean (ZERO_MEAN)."""
@@ -89,6 +90,7 @@ def problem(nx, ny, nz, bc, box=(0, 1, 0, 1, 0, 1), compat_zero_mode=1, dirichle
     p.compat_zero_mode = int(compat_zero_mode)
     p.dirichlet_lift = int(dirichlet_lift)
     p.zero_mean = int(zero_mean)
+    p.z_method = int(z_method)
     keep = []
     for f, g in (faces or {}).items():
         a = np.ascontiguousarray(g, dtype=np.float64).ravel()

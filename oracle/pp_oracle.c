@@ -559,6 +559,164 @@ static double exact_value(double omega, double x, int tg)
 /* ------------------------------------------------------------------------- */
 /* validation                                                                  */
 /* ------------------------------------------------------------------------- */
+/* ------------------------------------------------------------------------- */
+/* the reference's alternate z solvers as its CPU build computes them          */
+/* ------------------------------------------------------------------------- */
+/* myLog2 (src/mathFunction.cpp:36): log2 truncated to int */
+static int ref_log2(int x) { return (int)(log2((double)x)); }
+
+/* TriDiag::pcr (src/triDiag.cpp:1442-1542) is written for OpenACC, where each
+ * vector lane keeps its own copy of the gathered a0..d2; compiled for the CPU
+ * those are arrays of 20 entries indexed by i / VECLENGTH (256), so the first
+ * loop leaves in entry b the neighbours of the LAST row of block b, and the
+ * second loop updates every row of the block with them.  Defined (every read
+ * in bounds, every entry within the 20) for Dirichlet or Neumann ends and
+ * nz <= 256 not a power of two: one block, whose last row n - 1 always has
+ * both i - s >= 0 and i + s >= n. */
+int ppo_ref_pcr_defined(int nz, char z0, char z1)
+{
+    if ((z0 != 'D' && z0 != 'N') || (z1 != 'D' && z1 != 'N')) return 0;
+    return nz >= 3 && nz <= 256 && (nz & (nz - 1)) != 0;
+}
+
+static void ref_pcr(int n, double* a, double* c, double* d)
+{
+    const int level = ref_log2(n) + 1;
+    const int m = 256; /* VECLENGTH, src/include/params.h:56 */
+    double a0[20], a1[20], a2[20], c0[20], c1[20], c2[20], d0[20], d1[20], d2[20];
+    for (int p = 0; p < level; p++) {
+        const int s = 1 << p;
+        for (int i = 0; i < n; i++) {
+            const int index = i / m;
+            if (i - s < 0 && i + s < n) {
+                a0[index] = a[i]; a1[index] = 0.0; a2[index] = a[i + s];
+                c0[index] = c[i]; c1[index] = 0.0; c2[index] = c[i + s];
+                d0[index] = d[i]; d1[index] = 0.0; d2[index] = d[i + s];
+            } else if (i + s >= n && i - s >= 0) {
+                a0[index] = a[i]; a1[index] = a[i - s]; a2[index] = 0.0;
+                c0[index] = c[i]; c1[index] = c[i - s]; c2[index] = 0.0;
+                d0[index] = d[i]; d1[index] = d[i - s]; d2[index] = 0.0;
+            } else {
+                a0[index] = a[i]; a1[index] = a[i - s]; a2[index] = a[i + s];
+                c0[index] = c[i]; c1[index] = c[i - s]; c2[index] = c[i + s];
+                d0[index] = d[i]; d1[index] = d[i - s]; d2[index] = d[i + s];
+            }
+        }
+        for (int i = 0; i < n; i++) {
+            const int index = i / m;
+            const double r = 1. / (1. - a0[index] * c1[index] - c0[index] * a2[index]);
+            a[i] = -r * a0[index] * a1[index];
+            c[i] = -r * c0[index] * c2[index];
+            d[i] = r * (d0[index] - a0[index] * d1[index] - c0[index] * d2[index]);
+        }
+    }
+}
+
+/* solvePCR (src/pencilDcmp.cpp:5239-5270): the system divided by eig
+ * (fillInArrayContigNormalize :5320-5345, imposeBoundaryonContainer
+ * :5372-5401, offDiagNormalize :5406-5452, imposeBoundaryonOffDiag
+ * :5457-5481), then pcr; r in, solution out */
+static void ref_solve_pcr(double* r, double eig, int nz, char z0, char z1, double* lower, double* upper)
+{
+    const double eigInv = 1. / eig;
+    const double r0 = r[0], rn = r[nz - 1];
+    for (int k = 1; k < nz - 1; k++) r[k] = r[k] * eigInv;
+    if (z0 == 'D') r[0] = r0 / (eig - 1.);
+    if (z1 == 'D') r[nz - 1] = rn / (eig - 1.);
+    if (z0 == 'N') r[0] = r0 / (eig + 1.);
+    if (z1 == 'N') r[nz - 1] = rn / (eig + 1.);
+    for (int k = 1; k < nz; k++) lower[k] = eigInv;
+    for (int k = 0; k < nz - 1; k++) upper[k] = eigInv;
+    lower[0] = 0.0;
+    upper[nz - 1] = 0.0;
+    if (z0 == 'D') upper[0] = 1. / (eig - 1.);
+    if (z1 == 'D') lower[nz - 1] = 1. / (eig - 1.);
+    if (z0 == 'N') upper[0] = 1. / (eig + 1.);
+    if (z1 == 'N') lower[nz - 1] = 1. / (eig + 1.);
+    ref_pcr(nz, lower, upper, r);
+}
+
+/* TriDiag::crp (src/triDiag.cpp:1285-1437): cyclic reduction of the
+ * constant-coefficient system (diagonal 1, off-diagonals 1/eig) down to a
+ * 3 x 3 system, solved by the three-row Thomas (thomasLowMem
+ * src/triDiag.cpp:1891-1950 with b = 1), and back-substitution.  Defined for
+ * nz = 2^L - 1 with Dirichlet ends (the only ends solveCRP treats), L >= 2. */
+int ppo_ref_crp_defined(int nz, char z0, char z1)
+{
+    if (z0 != 'D' || z1 != 'D') return 0;
+    return nz >= 3 && nz <= 32767 && ((nz + 1) & nz) == 0;
+}
+
+static void ref_thomas3(const double* a, const double* b, const double* c, double* r)
+{
+    double gam[3], bet;
+    r[0] = r[0] / (bet = b[0]);
+    gam[1] = c[0] / bet;
+    bet = b[1] - a[1] * gam[1];
+    r[1] = (r[1] - a[1] * r[0]) / bet;
+    gam[2] = c[1] / bet;
+    bet = b[2] - a[2] * gam[2];
+    r[2] = (r[2] - a[2] * r[1]) / bet;
+    for (int j = 1; j >= 0; j--) r[j] -= gam[j + 1] * r[j + 1];
+}
+
+static void ref_crp(int n, double offdiag, double* rhs)
+{
+    const int level = ref_log2(n);
+    double tmpA[16], tmpC[16];
+    int m = n;
+    tmpA[0] = offdiag;
+    tmpC[0] = offdiag;
+    for (int i = 0; i < level - 1; i++) {
+        const int d1 = 1 << (i + 1);
+        m = m >> 1;
+        const double a0 = tmpA[i], c0 = tmpC[i];
+        const double cte = 1. - (2. * a0 * c0);
+        for (int j = 0; j < m; j++) {
+            const int ind0 = d1 * j + (d1 - 1);
+            const int im1 = d1 * j + (d1 - 1) - d1 / 2;
+            const int ip1 = d1 * j + (d1 - 1) + d1 / 2;
+            rhs[ind0] = (rhs[im1] * (-a0) + rhs[ind0] + rhs[ip1] * (-c0)) / cte;
+        }
+        tmpA[i + 1] = -a0 * a0 / cte;
+        tmpC[i + 1] = -c0 * c0 / cte;
+    }
+    {
+        const int d1 = 1 << level;
+        const int ind0 = d1 - 1, im1 = (d1 - 1) - d1 / 2, ip1 = (d1 - 1) + d1 / 2;
+        double t[3] = {rhs[im1], rhs[ind0], rhs[ip1]};
+        const double A[3] = {0.0, tmpA[level - 1], tmpA[level - 1]};
+        const double B[3] = {1.0, 1.0, 1.0};
+        const double C[3] = {tmpC[level - 1], tmpC[level - 1], 0.0};
+        ref_thomas3(A, B, C, t);
+        rhs[ind0] = t[1];
+        rhs[im1] = t[0];
+        rhs[ip1] = t[2];
+    }
+    m = 3;
+    for (int i = level - 1; i > 0; i--) {
+        const int d0 = 1 << i;
+        for (int j = 0; j < m; j++)
+            rhs[d0 * j + (d0 - 1) - d0 / 2] = rhs[d0 * j + (d0 - 1) - d0 / 2] - tmpA[i - 1] * rhs[d0 * j + (d0 - 1)];
+        for (int j = 0; j < m; j++)
+            rhs[d0 * j + (d0 - 1) + d0 / 2] = rhs[d0 * j + (d0 - 1) + d0 / 2] - tmpC[i - 1] * rhs[d0 * j + (d0 - 1)];
+        m = (1 << (level - i + 2)) - 1;
+    }
+}
+
+/* solveCRP (src/pencilDcmp.cpp:5275-5315): interior rows times 1/eig
+ * (fillInArrayContigNormalize), the Dirichlet end rows divided by eig
+ * (imposeBoundaryonCRPTmp :5350-5369), then crp with off-diagonal 1/eig */
+static void ref_solve_crp(double* r, double eig, int nz)
+{
+    const double eigInv = 1. / eig;
+    const double r0 = r[0], rn = r[nz - 1];
+    for (int k = 1; k < nz - 1; k++) r[k] = r[k] * eigInv;
+    r[0] = r0 / (eig);
+    r[nz - 1] = rn / (eig);
+    ref_crp(nz, 1. / eig, r);
+}
+
 int ppo_check(const ppo_problem* pb)
 {
     if (pb->nx < 2 || pb->ny < 2 || pb->nz < 3) return PPO_ERR_INPUT;
@@ -573,6 +731,9 @@ int ppo_check(const ppo_problem* pb)
     }
     for (int d = 0; d < 3; ++d)
         if (!(pb->box[2 * d + 1] > pb->box[2 * d])) return PPO_ERR_INPUT;
+    if (pb->z_method == 1 && !ppo_ref_pcr_defined(pb->nz, z0, z1)) return PPO_ERR_INPUT;
+    if (pb->z_method == 2 && !ppo_ref_crp_defined(pb->nz, z0, z1)) return PPO_ERR_INPUT;
+    if (pb->z_method < 0 || pb->z_method > 2) return PPO_ERR_INPUT;
     return 0;
 }
 
@@ -779,7 +940,11 @@ int ppo_solve(const ppo_problem* pb, const double* rhs_re, const double* rhs_im,
                 double eig = ppo_eigenvalue(pb, jx, iy);
                 for (int c = 0; c < nidx; ++c) {
                     for (int k = 0; k < nz; ++k) r[k] = AT(jx, iy, k, c);
-                    if (pb->bc[4] != 'P')
+                    if (pb->z_method == 1)
+                        ref_solve_pcr(r, eig, nz, pb->bc[4], pb->bc[5], g, r1);
+                    else if (pb->z_method == 2)
+                        ref_solve_crp(r, eig, nz);
+                    else if (pb->bc[4] != 'P')
                         thomas_low_mem(g, r, eig, nz, pb->bc[4], pb->bc[5], pin);
                     else
                         sherman_morrison(g, r, r1, eig, 1.0, 1.0, nz);

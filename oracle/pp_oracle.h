@@ -34,10 +34,16 @@ typedef struct {
      * stencil weight (dz/dx)^2, (dz/dy)^2 or 1. */
     const double* face[6];
     int zero_mean;        /* 1: the reference's ZERO_MEAN (subtractMeanValue) */
+    /* the reference's SOLUTIONMETHOD (src/pencilDcmp.cpp:6102-6148): 0 Thomas
+     * (default), 1 its normalised PCR, 2 its CR-P, as its CPU build computes
+     * them (ppo_check gives the sizes each is defined for) */
+    int z_method;
 } ppo_problem;
 
 int ppo_kind_from_bc(char lo, char hi);
 int ppo_check(const ppo_problem* pb);
+int ppo_ref_pcr_defined(int nz, char z0, char z1);
+int ppo_ref_crp_defined(int nz, char z0, char z1);
 double ppo_eigenvalue(const ppo_problem* pb, int kx, int ky);
 void ppo_dft(int n, int sign, double* re, double* im);
 void ppo_dirichlet_lift(const ppo_problem* pb, double* lift);

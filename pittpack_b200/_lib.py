@@ -20,6 +20,8 @@ PP_PRECISION_FP64 = 0
 PP_PRECISION_MIXED = 1
 PP_ZSOLVE_DIRECT = 0
 PP_ZSOLVE_MULTIGRID = 1
+PP_ZSOLVE_REF_PCR = 2
+PP_ZSOLVE_REF_CRP = 3
 
 
 class Options(ctypes.Structure):

@@ -214,3 +214,19 @@ int pp_zsolve_mg_levels_total(int nz);
 size_t pp_zsolve_mg_smem(int G, int nz, bool cplx);
 // cudaErrorInvalidValue when one system's levels do not fit shared memory
 cudaError_t pp_launch_zsolve_mg(PPZMgArgs a, bool cplx, cudaStream_t st);
+
+// the reference's alternate z solvers as its CPU build computes them
+// (pp_zsolve_ref.cu): method PP_ZSOLVE_REF_PCR or PP_ZSOLVE_REF_CRP on the
+// [k][ky][kx] spectrum (parts = 2: complex-interleaved), in place
+struct PPZRefArgs {
+    double* data;
+    int nx, ny, nz;   // spectrum columns, rows, planes
+    int parts;
+    const double* ax;
+    const double* ay;
+    double Cx, Cy;
+    int zlo, zhi;     // PP_Z_DIRICHLET / PP_Z_NEUMANN / PP_Z_PERIODIC
+    int method;
+};
+bool pp_zsolve_ref_defined(int method, int nz, int zlo, int zhi);
+cudaError_t pp_launch_zsolve_ref(const PPZRefArgs& a, cudaStream_t st);

@@ -834,6 +834,22 @@ int launch_solve(pp_solver_s* h)
         e = pp_launch_zsolve_mg(m, s_cplx, h->stream);
         if (e == cudaErrorInvalidValue) return PP_UNSUPPORTED;  // levels exceed shared memory
         if (e != cudaSuccess) return set_cuda_error(h, e, PP_THOMAS_FAIL);
+    } else if (h->opt.z_solver == PP_ZSOLVE_REF_PCR || h->opt.z_solver == PP_ZSOLVE_REF_CRP) {
+        PPZRefArgs r{};
+        r.data = z.data;
+        r.nx = ncol;
+        r.ny = ny;
+        r.nz = nz;
+        r.parts = s_cplx ? 2 : 1;
+        r.ax = z.ax;
+        r.ay = z.ay;
+        r.Cx = z.Cx;
+        r.Cy = z.Cy;
+        r.zlo = z.zlo;
+        r.zhi = z.zhi;
+        r.method = h->opt.z_solver;
+        if (!pp_zsolve_ref_defined(r.method, nz, r.zlo, r.zhi)) return PP_UNSUPPORTED;
+        if ((e = pp_launch_zsolve_ref(r, h->stream)) != cudaSuccess) return set_cuda_error(h, e, PP_THOMAS_FAIL);
     } else if ((e = pp_launch_zsolve(z, s_cplx, h->stream)) != cudaSuccess) {
         return set_cuda_error(h, e, PP_THOMAS_FAIL);
     }
@@ -1223,7 +1239,7 @@ int pp_set_options(pp_handle h, const pp_options* opt)
     if (!opt) return PP_INPUT_ARGS;
     if (opt->precision != PP_PRECISION_FP64 && opt->precision != PP_PRECISION_MIXED) return PP_INPUT_ARGS;
     if (opt->max_sweeps < 0 || opt->max_sweeps > 16) return PP_INPUT_ARGS;
-    if (opt->z_solver != PP_ZSOLVE_DIRECT && opt->z_solver != PP_ZSOLVE_MULTIGRID) return PP_INPUT_ARGS;
+    if (opt->z_solver < PP_ZSOLVE_DIRECT || opt->z_solver > PP_ZSOLVE_REF_CRP) return PP_INPUT_ARGS;
     if (opt->zero_mean != 0 && opt->zero_mean != 1) return PP_INPUT_ARGS;
     std::lock_guard<std::mutex> g(h->mu);
     const bool lift_changed = opt->dirichlet_lift != h->opt.dirichlet_lift;

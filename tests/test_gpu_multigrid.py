@@ -79,7 +79,7 @@ def test_multigrid_option_rules():
     with pp.make_Poisson(16, 16, 16) as M:
         M.assignBoundary("DDDDDD")
         with pytest.raises(pp.PittPackError) as e:
-            M.setOptions(z_solver=2)
+            M.setOptions(z_solver=4)  # 0..3: direct, multigrid, the two reference parity modes
         assert e.value.code == 19
         # the refined mixed-precision solve uses the direct z solve only
         M.setOptions(z_solver=1, precision=1)
