@@ -178,10 +178,11 @@ struct PPResidArgs {
 int pp_resid_tiles(int nx, int ny);
 cudaError_t pp_launch_resid(const PPResidArgs& a, cudaStream_t st);
 // The kx = ky = 0 column of a refined sweep from per-CTA partial sums
-// ([plane][tpp] each), added in a fixed order: zcol[k] = scale * sum_t
-// part[k tpp + t]; if upart is set, *usum = the sum of all of upart.
+// ([plane][tpp] each), added in a fixed order (one block per plane):
+// zcol[k] = scale * sum_t part[k tpp + t]; if upart is set, uplane[k] = the
+// plane's sum of upart and *usum = the sum of uplane (nz doubles of scratch).
 cudaError_t pp_launch_zero_mode_sums(const double* part, const double* upart, int tpp, int nz, double scale,
-                                     double* zcol, double* usum, cudaStream_t st);
+                                     double* zcol, double* usum, double* uplane, cudaStream_t st);
 // zero-mean solution (pp_mean.cu): the mean of the real parts of the n
 // complex-interleaved values of P is subtracted from them; scratch holds
 // pp_zero_mean_scratch_doubles() doubles

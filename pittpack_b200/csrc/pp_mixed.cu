@@ -304,30 +304,49 @@ __global__ void __launch_bounds__(RT_THREADS) resid_kernel(PPResidArgs a, int nt
     }
 }
 
-// zcol[k] = scale * (sum of the plane's partials in order); the sum of all
-// u partials in a fixed tree
-__global__ void zero_mode_sums_kernel(const double* part, const double* upart, int tpp, int nz, double scale,
-                                      double* zcol, double* usum)
+// the 256 threads' values added in a fixed tree; the total in red[0]
+PP_D void zm_tree(double* red)
 {
-    __shared__ double red[256];
-    double us = 0.0;
-    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
-        const double* p = part + (long)k * tpp;
-        double s = 0.0;
-        for (int t = 0; t < tpp; ++t) s += p[t];
-        zcol[k] = scale * s;
-        if (upart) {
-            const double* q = upart + (long)k * tpp;
-            for (int t = 0; t < tpp; ++t) us += q[t];
-        }
-    }
-    if (!upart) return;
-    red[threadIdx.x] = us;
     __syncthreads();
     for (int o = blockDim.x / 2; o > 0; o >>= 1) {
         if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
         __syncthreads();
     }
+}
+
+// one block per plane k: zcol[k] = scale * (the plane's partials: each
+// thread's stride-256 share in order, then a fixed tree); uplane[k] = the
+// plane's u partials alike
+__global__ void zero_mode_sums_kernel(const double* part, const double* upart, int tpp, double scale, double* zcol,
+                                      double* uplane)
+{
+    __shared__ double red[256], redu[256];
+    const int k = blockIdx.x;
+    const double* p = part + (long)k * tpp;
+    const double* q = upart ? upart + (long)k * tpp : nullptr;
+    double s = 0.0, us = 0.0;
+    for (int t = threadIdx.x; t < tpp; t += blockDim.x) {
+        s += p[t];
+        if (q) us += q[t];
+    }
+    red[threadIdx.x] = s;
+    redu[threadIdx.x] = us;
+    zm_tree(red);
+    if (q) zm_tree(redu);
+    if (threadIdx.x == 0) {
+        zcol[k] = scale * red[0];
+        if (q) uplane[k] = redu[0];
+    }
+}
+
+// *usum = the planes' u sums added in a fixed tree
+__global__ void zero_mode_usum_kernel(const double* uplane, int nz, double* usum)
+{
+    __shared__ double red[256];
+    double us = 0.0;
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) us += uplane[k];
+    red[threadIdx.x] = us;
+    zm_tree(red);
     if (threadIdx.x == 0) *usum = red[0];
 }
 
@@ -380,8 +399,11 @@ cudaError_t pp_launch_resid(const PPResidArgs& a, cudaStream_t st)
 }
 
 cudaError_t pp_launch_zero_mode_sums(const double* part, const double* upart, int tpp, int nz, double scale,
-                                     double* zcol, double* usum, cudaStream_t st)
+                                     double* zcol, double* usum, double* uplane, cudaStream_t st)
 {
-    zero_mode_sums_kernel<<<1, 256, 0, st>>>(part, upart, tpp, nz, scale, zcol, usum);
+    zero_mode_sums_kernel<<<nz, 256, 0, st>>>(part, upart, tpp, scale, zcol, uplane);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !upart) return e;
+    zero_mode_usum_kernel<<<1, 256, 0, st>>>(uplane, nz, usum);
     return cudaGetLastError();
 }

@@ -226,7 +226,7 @@ struct pp_solver_s {
     const double* ext_rhs = nullptr;
     double* ext_out = nullptr;
     pp_tuning tune{0, 0, 0};  // launch-shape choices (0 = built-in default)
-    DevBuf psum;   // refined solve: per-plane sums / zero-mode column (nz doubles)
+    DevBuf psum;   // refined solve: zero-mode column, sum of u, target mean, planes' sums of u (2 nz + 2 doubles)
     DevBuf part;   // refined solve: per-CTA partial sums of r and of u (2 x nz x tiles)
     DevBuf errc;   // CTAs whose bounded waits ran out (one int)
     DevBuf zero1;  // one double 0.0 (eigen table of the zero-mode system)
@@ -920,8 +920,9 @@ int launch_mixed(pp_solver_s* h)
     double* u = reinterpret_cast<double*>(h->bufB.as<char>() + h->bufB.bytes / 2);
     const int tpp = pp_resid_tiles(nx, ny);
     if (zm && !h->psum.p) {
-        // zero-mode column (nz) + sum of u + target mean
-        if ((e = h->psum.alloc(sizeof(double) * (nz + 2))) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
+        // zero-mode column (nz) + sum of u + target mean + the planes' sums of u (nz)
+        if ((e = h->psum.alloc(sizeof(double) * (2 * nz + 2))) != cudaSuccess)
+            return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
         if ((e = h->zero1.alloc(sizeof(double))) != cudaSuccess) return set_cuda_error(h, e, PP_ALLOCATION_FAIL);
         if ((e = cudaMemset(h->zero1.p, 0, sizeof(double))) != cudaSuccess) return set_cuda_error(h, e, PP_CUDA_ERROR);
     }
@@ -1029,7 +1030,7 @@ int launch_mixed(pp_solver_s* h)
             t0 = stamp(h);
             double* ps = h->psum.as<double>();
             if ((e = pp_launch_zero_mode_sums(part, want_usum ? upart : nullptr, tpp, nz, psum_scale, ps, ps + nz,
-                                              h->stream)) != cudaSuccess)
+                                              ps + nz + 2, h->stream)) != cudaSuccess)
                 return set_cuda_error(h, e, PP_CUDA_ERROR);
             if ((e = pp_launch_zsolve(z0, false, h->stream)) != cudaSuccess) return set_cuda_error(h, e, PP_THOMAS_FAIL);
             if (singular &&
