@@ -20,7 +20,8 @@ the solver stream, max over ranks); `e2e` times the public API end to end:
 per grid, page-locked host RHS -> pp_assign_rhs_async (H2D) -> pp_solve ->
 pp_get_solution_real_async (D2H of the solution's real part: the RHS is real,
 so the imaginary part is zero), the four grids on four streams so that their
-copies overlap, wall clock until every stream has finished; the same with
+copies overlap, the steps issued back to back (a step's downloads overlap
+the next step's uploads), wall clock until every stream has finished; the same with
 the complex-interleaved chunkedArray P (pp_get_solution_async, twice the
 bytes down) is reported beside it.  Inputs (1 GiB per grid) are larger than
 the 126 MB L2, so no flush is needed between solves.
@@ -826,18 +827,26 @@ def run_ours(args):
                 M.getSolutionRealAsync(o)
             else:
                 M.getSolutionAsync(oc)
+
+    def e2e_wait():
         for M in solvers:
             M.synchronize()
 
+    # the steps are issued back to back on the grids' streams (each stream
+    # runs upload, solve, download of its grid in order), so one step's
+    # downloads overlap the next step's uploads; every step's copies are in
+    # the timed region, which ends when the last download has landed
     e2e = {}
     for real in (True, False):
         e2e_step(real)  # warm-up of the copy path
+        e2e_wait()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         w0 = time.perf_counter()
         for _ in range(e2e_steps):
             e2e_step(real)
+        e2e_wait()
         torch.cuda.synchronize()
         e2e_s = max_over_ranks(time.perf_counter() - w0, dist, "cuda")
         e2e["real" if real else "complex"] = replica_throughput(world, e2e_steps * len(FAMILIES) * npts, e2e_s)
