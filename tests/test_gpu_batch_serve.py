@@ -141,3 +141,31 @@ def test_server_rejects_a_request_that_never_fits():
     st, _, _ = S.wait(S.submit(16, 16, 16, "DDDDDD", rhs, P))
     assert st == 15  # ALLOCATION_FAIL
     S.close()
+
+
+def test_batch_with_chirp_and_long_line_grids():
+    """Grids whose x length takes the chirp z-transform (131) or the
+    four-step path (8192, 7500) in one graph with an ordinary grid: their
+    scratch is set up by the first solve, outside the capture."""
+    import torch
+
+    from pittpack_b200.batch import Batch
+
+    rng = np.random.default_rng(17)
+    shapes = [(131, 16, 8, "NNDDDD"), (8192, 4, 3, "DDDDDD"), (7500, 4, 3, "NNNNDD"), (40, 40, 20, "DDDDNN")]
+    grids, items, outs = [], [], []
+    for nx, ny, nz, bc in shapes:
+        f = rng.standard_normal((nz, ny, nx))
+        grids.append((nx, ny, nz, bc, f))
+        d_rhs = torch.from_numpy(f.ravel().copy()).cuda()
+        d_P = torch.empty(2 * f.size, dtype=torch.float64, device="cuda")
+        items.append(dict(nx=nx, ny=ny, nz=nz, bc=bc, d_rhs=d_rhs.data_ptr(), d_P=d_P.data_ptr()))
+        outs.append((d_rhs, d_P))
+    for precision in (0, 1):
+        B = Batch(items, precision=precision, sweeps=2, branches=4, autotune=False)
+        B.run(torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        for grid, (_, d_P) in zip(grids, outs):
+            nx, ny, nz = grid[:3]
+            _check(d_P.cpu().numpy().view(np.complex128).reshape(nz, ny, nx), grid, precision)
+        B.close()
