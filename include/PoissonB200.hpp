@@ -62,12 +62,9 @@ class PoissonB200 {
     // the reference's analytic RHS, -4 pi^2 cos(2 pi z) at the cell centres
     // (src/pencilDcmp.cpp:5685-5759): nx*ny*nz doubles
     void fillTrigonometric(double* rhs) { check(pp_fill_trigonometric(h_, rhs), "fillTrigonometric"); }
-    // the reference's HDF5 writer is not part of this library: read P with
-    // getSolution() and write it with the caller's own tools
-    void IO(int /*app*/, int /*dir*/, int /*aligndir*/)
-    {
-        throw Error(PP_UNSUPPORTED, "IO: HDF5 output is not provided; read P with getSolution()");
-    }
+    // the reference's writer: soln/Pxdmf3d<app>.xmf (XDMF, the real part of P
+    // as a raw float64 Binary data item beside it; no HDF5 library needed)
+    void IO(int app, int dir, int aligndir) { check(pp_io(h_, (unsigned)app, dir, aligndir), "IO"); }
     void setOptions(const pp_options& o) { check(pp_set_options(h_, &o), "setOptions"); }
     pp_options options() const
     {

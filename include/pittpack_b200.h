@@ -178,6 +178,18 @@ int pp_get_solution_async(pp_handle h, double* P);
  * counterpart in the reference, which leaves the complex P in host memory. */
 int pp_get_solution_real(pp_handle h, double* u);
 int pp_get_solution_real_async(pp_handle h, double* u);
+/* PencilDcmp::IO (src/pencilDcmp.cpp:1827-1832): the solution for ParaView /
+ * VisIt as soln/Pxdmf3d<app>.xmf, the reference's XDMF file name, with its
+ * Collection "AMR" of one Uniform grid "mesh0" and the real part of P as the
+ * cell-centred attribute "Q" (Phdf5::writeMultiBlockCellCenter,
+ * src/phdf5.cpp:1299-1808).  No HDF5 library is required: Q is a raw
+ * little-endian float64 file, soln/Pxdmf3d<app>_Q.bin ([k][j][i], i fastest),
+ * referenced as an XDMF Binary data item, and the uniform grid is a
+ * 3DCoRectMesh with origin and spacing instead of X/Y/Z node arrays.  One
+ * block at one rank: dir and aligndir (0..2), which order the reference's
+ * pencil chunks, do not change it.  soln/ is created when absent.  Returns
+ * PP_NOT_READY before a solve, PP_INPUT_ARGS when a file cannot be written. */
+int pp_io(pp_handle h, unsigned app, int dir, int aligndir);
 
 /* getError (src/pencilDcmp.cpp:2040-2208): RMS error of the solution against
  * the reference's manufactured solution; does not modify the solution */

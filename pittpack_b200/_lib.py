@@ -84,6 +84,7 @@ def load():
         "pp_get_error_manufactured": ([H, dp], i),
         "pp_fill_trigonometric": ([H, ctypes.c_void_p], i),
         "pp_fill_trigonometric_box": ([i, i, i, dp, ctypes.c_void_p], i),
+        "pp_io": ([ctypes.c_void_p, ctypes.c_uint, i, i], i),
         "pp_zsolve_stats": ([H, ctypes.POINTER(i), ctypes.POINTER(i)], i),
         "pp_set_stream": ([H, ctypes.c_void_p], i),
         "pp_synchronize": ([H], i),

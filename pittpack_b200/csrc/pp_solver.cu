@@ -2,6 +2,7 @@
 // of one solve, and the C ABI declared in include/pittpack_b200.h.
 #include <algorithm>
 #include <cmath>
+#include <cerrno>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -9,6 +10,8 @@
 #include <new>
 #include <string>
 #include <vector>
+
+#include <sys/stat.h>
 
 #include "../../include/pittpack_b200.h"
 #include "pp_common.cuh"
@@ -217,6 +220,7 @@ struct pp_solver_s {
     double box[6] = {0, 1, 0, 1, 0, 1};
     char bc[6] = {0};
     bool have_bc = false, have_rhs = false, rhs_complex = false;
+    bool solved = false;  // a solve has been issued (the solution buffer holds one)
     pp_options opt{};
     cudaStream_t stream = 0;
     DirTables tx, ty;
@@ -1362,6 +1366,7 @@ int pp_solve(pp_handle h)
     if (h->timing) h->tcount++;
     const int rc = h->opt.precision == PP_PRECISION_MIXED ? launch_mixed(h) : launch_solve(h);
     h->timing = false;
+    if (rc == PP_SUCCESS) h->solved = true;
     return rc;
 }
 
@@ -1466,6 +1471,55 @@ static int get_real(pp_handle h, double* u, bool wait)
 }
 
 int pp_get_solution_real(pp_handle h, double* u) { return get_real(h, u, true); }
+
+int pp_io(pp_handle h, unsigned app, int dir, int aligndir)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (dir < 0 || dir > 2 || aligndir < 0 || aligndir > 2) return PP_INPUT_ARGS;
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    double box[6];
+    {
+        std::lock_guard<std::mutex> g(h->mu);
+        if (!h->solved) return PP_NOT_READY;
+        std::memcpy(box, h->box, sizeof box);
+    }
+    std::vector<double> q((size_t)nx * ny * nz);
+    const int rc = pp_get_solution_real(h, q.data());
+    if (rc != PP_SUCCESS) return rc;
+    if (mkdir("soln", 0755) != 0 && errno != EEXIST) return PP_INPUT_ARGS;
+    char base[64], path[96];
+    std::snprintf(base, sizeof base, "Pxdmf3d%u", app);
+    // the attribute values, little-endian float64 (the host's order on x86-64 / aarch64)
+    std::snprintf(path, sizeof path, "soln/%s_Q.bin", base);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return PP_INPUT_ARGS;
+    const size_t wrote = std::fwrite(q.data(), sizeof(double), q.size(), f);
+    if (std::fclose(f) != 0 || wrote != q.size()) return PP_INPUT_ARGS;
+    std::snprintf(path, sizeof path, "soln/%s.xmf", base);
+    f = std::fopen(path, "w");
+    if (!f) return PP_INPUT_ARGS;
+    const double dx = (box[1] - box[0]) / nx, dy = (box[3] - box[2]) / ny, dz = (box[5] - box[4]) / nz;
+    int bad = 0;
+    bad |= std::fprintf(f, "<?xml version=\"1.0\" ?>\n<!DOCTYPE Xdmf SYSTEM \"Xdmf.dtd\" []>\n") < 0;
+    bad |= std::fprintf(f, "<Xdmf Version=\"2.0\">\n<Domain>\n") < 0;
+    bad |= std::fprintf(f, "<Grid Name=\"AMR\" GridType=\"Collection\" CollectionType=\"Spatial\">\n") < 0;
+    bad |= std::fprintf(f, "  <Grid Name=\"mesh0\" GridType=\"Uniform\">\n") < 0;
+    bad |= std::fprintf(f, "    <Topology TopologyType=\"3DCoRectMesh\" Dimensions=\"%d %d %d\"/>\n", nz + 1, ny + 1,
+                        nx + 1) < 0;
+    // XDMF lists a CoRectMesh's origin and spacing slowest axis first (z y x)
+    bad |= std::fprintf(f, "    <Geometry GeometryType=\"ORIGIN_DXDYDZ\">\n") < 0;
+    bad |= std::fprintf(f, "      <DataItem Dimensions=\"3\" NumberType=\"Float\" Precision=\"8\" Format=\"XML\">"
+                           "%.17g %.17g %.17g</DataItem>\n", box[4], box[2], box[0]) < 0;
+    bad |= std::fprintf(f, "      <DataItem Dimensions=\"3\" NumberType=\"Float\" Precision=\"8\" Format=\"XML\">"
+                           "%.17g %.17g %.17g</DataItem>\n", dz, dy, dx) < 0;
+    bad |= std::fprintf(f, "    </Geometry>\n") < 0;
+    bad |= std::fprintf(f, "    <Attribute Name=\"Q\" AttributeType=\"Scalar\" Center=\"Cell\">\n") < 0;
+    bad |= std::fprintf(f, "      <DataItem Dimensions=\"%d %d %d\" NumberType=\"Float\" Precision=\"8\" "
+                           "Format=\"Binary\" Endian=\"Little\">%s_Q.bin</DataItem>\n", nz, ny, nx, base) < 0;
+    bad |= std::fprintf(f, "    </Attribute>\n  </Grid>\n</Grid>\n</Domain>\n</Xdmf>\n") < 0;
+    if (std::fclose(f) != 0 || bad) return PP_INPUT_ARGS;
+    return PP_SUCCESS;
+}
 int pp_get_solution_real_async(pp_handle h, double* u) { return get_real(h, u, false); }
 
 int pp_get_solution_device(pp_handle h, double* d_P)

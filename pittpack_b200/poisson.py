@@ -101,9 +101,10 @@ class PoissonGPU:
         return rhs
 
     def IO(self, app: int = 1, dir: int = 2, aligndir: int = 0) -> None:  # noqa: A002 - the reference's names
-        """The reference's HDF5/XDMF writer (src/pencilDcmp.cpp:1827-1832 ->
-        src/phdf5.cpp) is not part of this library: read P with getSolution()."""
-        raise PittPackError(_lib.PP_UNSUPPORTED, "IO: HDF5 output is not provided; read P with getSolution()")
+        """The reference's writer (src/pencilDcmp.cpp:1827-1832): the real part
+        of P as soln/Pxdmf3d<app>.xmf with a raw float64 data file beside it
+        (XDMF Binary item; no HDF5 library needed)."""
+        check(self._L.pp_io(self._h, int(app), int(dir), int(aligndir)), "IO")
 
     def options(self) -> Options:
         o = Options()

@@ -4,7 +4,8 @@ src/main.cpp:115 passes to assignRhs.  The library's host function
 (pp_fill_trigonometric_box, no GPU needed) is checked bit for bit against the
 reference's own build (oracle/_ref/libppref.so) and against the formula; the
 facade methods that have nothing to do at one rank (constructConnectivity,
-graphCreate, readIn) and the HDF5 writer IO (not provided) are checked too."""
+graphCreate, readIn) and the writer IO (which needs a solved handle) are
+checked too."""
 import ctypes
 import os
 
@@ -68,6 +69,7 @@ def _solver(nx, ny, nz, box):
     M.nx, M.ny, M.nz = nx, ny, nz
     M._box = np.array(box, dtype=np.float64)
     M.bc = None
+    M._h = None  # no device handle: this test runs without a GPU
     return M
 
 
@@ -84,5 +86,5 @@ def test_facade_follows_the_reference_driver():
         M.fillTrigonometric(np.empty(nx * ny * nz, dtype=np.float32))
     assert e.value.code == _lib.PP_INPUT_ARGS
     with pytest.raises(PittPackError) as e:
-        M.IO(1, 2, 0)
-    assert e.value.code == _lib.PP_UNSUPPORTED
+        M.IO(1, 2, 0)  # the writer needs a solved handle
+    assert e.value.code == _lib.PP_INVALID_HANDLE
