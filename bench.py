@@ -358,6 +358,50 @@ def run_batch_leg(args, torch, stream):
             "mode": best, "modes": res}
 
 
+def run_slab_leg(args, torch, dist, nx, ny, nz, bc):
+    """One grid solved as z slabs over the N ranks (pittpack_b200.distributed:
+    two all-to-all exchanges per solve, NCCL on device tensors): Mpoints/s of
+    that one grid, timed by the slowest rank around K synchronised solves
+    (strong scaling), and the rel. L2 of the assembled solution against each
+    rank's whole-grid solve on its own GPU."""
+    import pittpack_b200 as pp
+    from pittpack_b200.distributed import SlabPoisson, _DevArray
+
+    g = torch.Generator(device="cuda").manual_seed(4242)
+    f = torch.randn((nz, ny, nx), dtype=torch.float64, device="cuda", generator=g)
+    world = dist.get_world_size()
+    with SlabPoisson(nx, ny, nz, bc) as S:
+        fl = f[S.k0:S.k0 + S.nzl].contiguous()
+        for _ in range(max(3, args.warmup)):
+            S.solve(fl, to_host=False)
+        torch.cuda.synchronize()
+        dist.barrier()
+        reps = max(3, min(args.steps, 10))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            S.solve(fl, to_host=False)
+        torch.cuda.synchronize()
+        sec = max_over_ranks(time.perf_counter() - t0, dist, "cuda") / reps
+        mine = S.solution_device().clone()
+        k0, nzl = S.k0, S.nzl
+    with pp.make_Poisson(nx, ny, nz) as W:
+        W.assignBoundary(bc)
+        W.assignRhsDevice(f.data_ptr(), False)
+        W.pittPack()
+        W.synchronize()
+        whole = torch.as_tensor(_DevArray(W.solutionDevicePtr(), 2 * nx * ny * nz), device="cuda")
+        whole = whole.view(torch.complex128).view(nz, ny, nx)[k0:k0 + nzl]
+        sums = torch.stack([torch.linalg.norm(mine - whole) ** 2, torch.linalg.norm(whole) ** 2])
+    dist.all_reduce(sums)
+    return {"workload": f"one {nx}x{ny}x{nz} {bc} grid as z slabs over {world} GPUs "
+                        "(forward transforms, all-to-all, z solve, all-to-all, inverse transforms)",
+            "value": nx * ny * nz / sec / 1e6, "unit": "Mpoints/s", "ms_per_solve": sec * 1e3,
+            "scaling": "strong", "steps": reps,
+            "rel_l2_vs_single_gpu": float((sums[0] / sums[1]).sqrt()),
+            "exchange": "NCCL all_to_all_single, twice per solve",
+            "timing": "wall clock around synchronised solves, max over ranks"}
+
+
 def run_serve_leg(args):
     """Poisson arrivals of single solves (seed 11) at each rate; host RHS in
     page-locked memory -> server (H2D, solve, D2H on one of 8 streams) -> host
@@ -856,7 +900,9 @@ def run_ours(args):
         M.close()
     del h_rhs, h_out, h_outc, ref_buf, mix_buf
     torch.cuda.empty_cache()
-    batch = serve = None
+    batch = serve = slab = None
+    if world > 1 and not args.no_slab:
+        slab = run_slab_leg(args, torch, dist, nx, ny, nz, FAMILIES[1 if len(FAMILIES) > 1 else 0])
     if world == 1 and not args.no_batch:
         batch = run_batch_leg(args, torch, stream)
     if world == 1 and not args.no_serve:
@@ -891,6 +937,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "batch": batch,
             "serving": serve,
+            "slab": slab,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -911,6 +958,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--sweeps", type=int, default=1, help="refinement sweeps of the mixed-precision mode")
     ap.add_argument("--no-batch", action="store_true", help="skip the 96-grid batched workload")
+    ap.add_argument("--no-slab", action="store_true",
+                    help="skip the one-grid slab-decomposed solve over the ranks (N > 1 only)")
     ap.add_argument("--no-serve", action="store_true", help="skip the request-stream workload")
     ap.add_argument("--serve-requests", type=int, default=160, help="requests per arrival rate")
     args = ap.parse_args()

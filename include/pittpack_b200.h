@@ -191,6 +191,31 @@ int pp_get_solution_real_async(pp_handle h, double* u);
  * PP_NOT_READY before a solve, PP_INPUT_ARGS when a file cannot be written. */
 int pp_io(pp_handle h, unsigned app, int dir, int aligndir);
 
+/* Staged solve of one z-slab of a grid decomposed over several GPUs (the
+ * reference's pencil decomposition, src/pencilDcmp.cpp:851-1825, as z slabs:
+ * a rank holds planes k0 .. k0 + nz_local - 1).  The handle is created for
+ * the slab (pp_create(nx, ny, nz_local)) with the slab's own z extent as its
+ * box, the same boundary letters as the whole grid, and pp_set_slab, which
+ * says whether the slab owns the grid's z-min / z-max faces (only those take
+ * the Dirichlet lift).  Then, for each solve:
+ *   pp_stage_forward     x and y transforms of the assigned RHS into the
+ *                        slab's spectrum, [k][ky][col] with pp_stage_spectrum's
+ *                        col count and doubles per point (2: complex);
+ *   (caller)             gather, for its share of spectrum rows ky = j0 ..
+ *                        j0 + rows - 1, every slab's planes into one array
+ *                        [k][ky - j0][col] (an all-to-all), k over the grid;
+ *   pp_stage_zsolve      the z solve of those columns, in place;
+ *   (caller)             scatter them back (the reverse all-to-all);
+ *   pp_stage_inverse     inverse y and x transforms into the slab's P.
+ * All launches go to the handle's stream.  Plain FP64 solve with the direct
+ * z solve; pp_solve on a slab handle returns PP_UNSUPPORTED.
+ * pittpack_b200/distributed.py does the exchanges with torch.distributed. */
+int pp_set_slab(pp_handle h, int owns_zmin, int owns_zmax);
+int pp_stage_forward(pp_handle h);
+int pp_stage_spectrum(pp_handle h, double** d_spec, int* ncol, int* parts);
+int pp_stage_zsolve(pp_handle h, double* d_cols, int nz_total, int rows, int j0);
+int pp_stage_inverse(pp_handle h);
+
 /* getError (src/pencilDcmp.cpp:2040-2208): RMS error of the solution against
  * the reference's manufactured solution; does not modify the solution */
 int pp_get_error_manufactured(pp_handle h, double* err);

@@ -85,6 +85,11 @@ def load():
         "pp_fill_trigonometric": ([H, ctypes.c_void_p], i),
         "pp_fill_trigonometric_box": ([i, i, i, dp, ctypes.c_void_p], i),
         "pp_io": ([ctypes.c_void_p, ctypes.c_uint, i, i], i),
+        "pp_set_slab": ([H, i, i], i),
+        "pp_stage_forward": ([H], i),
+        "pp_stage_spectrum": ([H, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(i), ctypes.POINTER(i)], i),
+        "pp_stage_zsolve": ([H, ctypes.c_void_p, i, i, i], i),
+        "pp_stage_inverse": ([H], i),
         "pp_zsolve_stats": ([H, ctypes.POINTER(i), ctypes.POINTER(i)], i),
         "pp_set_stream": ([H, ctypes.c_void_p], i),
         "pp_synchronize": ([H], i),

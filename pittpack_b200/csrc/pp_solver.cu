@@ -221,6 +221,10 @@ struct pp_solver_s {
     char bc[6] = {0};
     bool have_bc = false, have_rhs = false, rhs_complex = false;
     bool solved = false;  // a solve has been issued (the solution buffer holds one)
+    // a z-slab of a grid decomposed over several GPUs (pp_set_slab): the
+    // staged entry points run, the z faces the slab does not own take no lift,
+    // and the spectrum keeps the usual [k][ky][kx] layout
+    bool slab = false, zface_lo = true, zface_hi = true;
     pp_options opt{};
     cudaStream_t stream = 0;
     DirTables tx, ty;
@@ -435,6 +439,7 @@ int build_lift(pp_solver_s* h)
         for (int slot = 0; slot < 6; ++slot) {
             const int f = face_of_slot[slot];
             if (h->bc[f] != 'D' || !h->uface[f].empty()) continue;
+            if ((slot == 0 && !h->zface_lo) || (slot == 1 && !h->zface_hi)) continue;  // inside a decomposed grid
             int na, nb;
             pp_mms_face_dims(mp, slot, &na, &nb);
             std::vector<double> v((size_t)na * nb);
@@ -452,6 +457,7 @@ int build_lift(pp_solver_s* h)
         const double hh[3] = {c1, c2, c3};
         for (int f = 0; f < 6; ++f) {
             if (h->uface[f].empty() || h->bc[f] == 'P') continue;
+            if ((f == 4 && !h->zface_lo) || (f == 5 && !h->zface_hi)) continue;  // inside a decomposed grid
             const int d = f / 2;
             const double c = h->bc[f] == 'D' ? 2.0 * wgt[d] : wgt[d] * hh[d];
             std::vector<double> v(h->uface[f].size());
@@ -662,7 +668,7 @@ int reg_lines(int n)
 }
 int z_tile_width(const pp_solver_s* h, bool s_cplx, int ncol)
 {
-    if (h->opt.z_solver != PP_ZSOLVE_DIRECT) return 0;
+    if (h->opt.z_solver != PP_ZSOLVE_DIRECT || h->slab) return 0;
     const int lpc = reg_lines(h->ny);
     if (lpc == 0) return 0;
     const int dl = s_cplx ? lpc : 2 * lpc;
@@ -727,7 +733,15 @@ int ensure_long_scratch(pp_solver_s* h)
     return PP_SUCCESS;
 }
 
-int launch_solve(pp_solver_s* h)
+// the z solve of a staged (slab) solve: gathered columns [nz][rows][ncol] of
+// spectrum rows j0 .. j0 + rows - 1
+struct StageZ {
+    double* data;
+    int nz, rows, j0;
+};
+enum { STAGE_FWD = 1, STAGE_Z = 2, STAGE_INV = 4, STAGE_ALL = 7 };
+
+int launch_solve(pp_solver_s* h, int stages = STAGE_ALL, const StageZ* sz = nullptr)
 {
     if (const int rc = ensure_long_scratch(h)) return rc;
     const int nx = h->nx, ny = h->ny, nz = h->nz;
@@ -774,6 +788,8 @@ int launch_solve(pp_solver_s* h)
     ay.L = tuned_lines(h, ay.fft.n);
     ay.tiles_per_plane = (ncol + ay.L - 1) / ay.L;
 
+    const int zt = z_tile_width(h, s_cplx, ncol);
+    if (stages & STAGE_FWD) {
     // forward x: rhs -> A
     PPLinePassArgs a1 = ax;
     a1.src = h->ext_rhs ? h->ext_rhs : h->rhs.as<double>();
@@ -789,25 +805,27 @@ int launch_solve(pp_solver_s* h)
     PPLinePassArgs a2 = ay;
     a2.src = h->bufA.as<double>();
     a2.dst = h->bufB.as<double>();
-    const int zt = z_tile_width(h, s_cplx, ncol);
     if (zt) set_z_tiled_out(a2, ncol, nz, zt);
     t0 = stamp(h);
     if ((e = line_pass(a2, h->ty, false, true, x_cplx, s_cplx, h->stream)) != cudaSuccess)
         return set_cuda_error(h, e, PP_CUFFT_FAIL_Y);
     stage_done(h, SLOT_YF, t0);
-    // z solve in B
+    }
+    if (stages & STAGE_Z) {
+    // z solve in B, or (staged) in the gathered columns of several slabs
+    const int zny = sz ? sz->rows : ny, znz = sz ? sz->nz : nz;
     PPZArgs z{};
-    z.data = h->bufB.as<double>();
+    z.data = sz ? sz->data : h->bufB.as<double>();
     z.nx = ncol;
-    z.ny = ny;
-    z.nz = nz;
+    z.ny = zny;
+    z.nz = znz;
     int zthreads = 0;
-    pp_zsolve_config_p(nz, s_cplx, ncol, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile, ny);
+    pp_zsolve_config_p(znz, s_cplx, ncol, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile, zny);
     z.P = h->tune.zsolve_lanes;
     z.tiled = zt ? 1 : 0;
     z.tiles_x = (ncol + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
-    z.ay = h->ty.eig.as<double>();
+    z.ay = h->ty.eig.as<double>() + (sz ? sz->j0 : 0);
     const double dx = -(h->box[0] - h->box[1]) / (nx);
     const double dy = -(h->box[2] - h->box[3]) / (ny);
     z.Cx = (dz / dx) * (dz / dx);
@@ -824,8 +842,8 @@ int launch_solve(pp_solver_s* h)
         PPZMgArgs m{};
         m.data = z.data;
         m.nx = ncol;
-        m.ny = ny;
-        m.nz = nz;
+        m.ny = zny;
+        m.nz = znz;
         m.ax = z.ax;
         m.ay = z.ay;
         m.Cx = z.Cx;
@@ -842,8 +860,8 @@ int launch_solve(pp_solver_s* h)
         PPZRefArgs r{};
         r.data = z.data;
         r.nx = ncol;
-        r.ny = ny;
-        r.nz = nz;
+        r.ny = zny;
+        r.nz = znz;
         r.parts = s_cplx ? 2 : 1;
         r.ax = z.ax;
         r.ay = z.ay;
@@ -852,12 +870,14 @@ int launch_solve(pp_solver_s* h)
         r.zlo = z.zlo;
         r.zhi = z.zhi;
         r.method = h->opt.z_solver;
-        if (!pp_zsolve_ref_defined(r.method, nz, r.zlo, r.zhi)) return PP_UNSUPPORTED;
+        if (!pp_zsolve_ref_defined(r.method, znz, r.zlo, r.zhi)) return PP_UNSUPPORTED;
         if ((e = pp_launch_zsolve_ref(r, h->stream)) != cudaSuccess) return set_cuda_error(h, e, PP_THOMAS_FAIL);
     } else if ((e = pp_launch_zsolve(z, s_cplx, h->stream)) != cudaSuccess) {
         return set_cuda_error(h, e, PP_THOMAS_FAIL);
     }
     stage_done(h, SLOT_Z, t0);
+    }
+    if (!(stages & STAGE_INV)) return PP_SUCCESS;
     // inverse y: B -> A
     PPLinePassArgs a3 = ay;
     a3.src = h->bufB.as<double>();
@@ -1361,11 +1381,81 @@ int pp_solve(pp_handle h)
     if (!h) return PP_INVALID_HANDLE;
     std::lock_guard<std::mutex> g(h->mu);
     if (!h->have_bc || !h->have_rhs) return PP_NOT_READY;
+    if (h->slab) return PP_UNSUPPORTED;  // a slab solves through the staged entry points
     cudaSetDevice(h->device);
     h->timing = h->tcount < h->tmax;
     if (h->timing) h->tcount++;
     const int rc = h->opt.precision == PP_PRECISION_MIXED ? launch_mixed(h) : launch_solve(h);
     h->timing = false;
+    if (rc == PP_SUCCESS) h->solved = true;
+    return rc;
+}
+
+// ---- staged solve of a z-slab (a grid decomposed over several GPUs) ---------------
+int pp_set_slab(pp_handle h, int owns_zmin, int owns_zmax)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    std::lock_guard<std::mutex> g(h->mu);
+    h->slab = true;
+    h->zface_lo = owns_zmin != 0;
+    h->zface_hi = owns_zmax != 0;
+    if (!h->have_bc) return PP_SUCCESS;
+    cudaSetDevice(h->device);
+    return build_lift(h);
+}
+
+static int stage_ready(pp_solver_s* h)
+{
+    if (!h->slab) return PP_INPUT_ARGS;
+    if (!h->have_bc) return PP_NOT_READY;
+    // the staged solve is the plain FP64 solve with the direct z solve
+    if (h->opt.precision != PP_PRECISION_FP64 || h->opt.z_solver != PP_ZSOLVE_DIRECT || h->opt.zero_mean)
+        return PP_UNSUPPORTED;
+    return PP_SUCCESS;
+}
+
+int pp_stage_forward(pp_handle h)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    std::lock_guard<std::mutex> g(h->mu);
+    if (const int rc = stage_ready(h)) return rc;
+    if (!h->have_rhs) return PP_NOT_READY;
+    cudaSetDevice(h->device);
+    return launch_solve(h, STAGE_FWD);
+}
+
+int pp_stage_spectrum(pp_handle h, double** d_spec, int* ncol, int* parts)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    if (!d_spec || !ncol || !parts) return PP_INPUT_ARGS;
+    std::lock_guard<std::mutex> g(h->mu);
+    if (const int rc = stage_ready(h)) return rc;
+    const int hc = half_spectrum_cols(h);
+    *d_spec = h->bufB.as<double>();
+    *ncol = hc ? hc : h->nx;
+    *parts = h->ty.kind == PP_KIND_FFT ? 2 : 1;
+    return PP_SUCCESS;
+}
+
+int pp_stage_zsolve(pp_handle h, double* d_cols, int nz_total, int rows, int j0)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    std::lock_guard<std::mutex> g(h->mu);
+    if (const int rc = stage_ready(h)) return rc;
+    if (!d_cols || nz_total < 3 || rows < 1 || j0 < 0 || j0 + rows > h->ny) return PP_INPUT_ARGS;
+    if (nz_total > pp_zsolve_max_nz(h->ty.kind == PP_KIND_FFT, false)) return PP_UNSUPPORTED;
+    cudaSetDevice(h->device);
+    const StageZ sz{d_cols, nz_total, rows, j0};
+    return launch_solve(h, STAGE_Z, &sz);
+}
+
+int pp_stage_inverse(pp_handle h)
+{
+    if (!h) return PP_INVALID_HANDLE;
+    std::lock_guard<std::mutex> g(h->mu);
+    if (const int rc = stage_ready(h)) return rc;
+    cudaSetDevice(h->device);
+    const int rc = launch_solve(h, STAGE_INV);
     if (rc == PP_SUCCESS) h->solved = true;
     return rc;
 }
