@@ -398,7 +398,7 @@ def run_slab_leg(args, torch, dist, nx, ny, nz, bc):
             "value": nx * ny * nz / sec / 1e6, "unit": "Mpoints/s", "ms_per_solve": sec * 1e3,
             "scaling": "strong", "steps": reps,
             "rel_l2_vs_single_gpu": float((sums[0] / sums[1]).sqrt()),
-            "exchange": "NCCL all_to_all_single, twice per solve",
+            "exchange": f"{dist.get_backend()} all_to_all_single, twice per solve",
             "timing": "wall clock around synchronised solves, max over ranks"}
 
 
@@ -660,8 +660,14 @@ def run_ours(args):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local_rank))
+        # NCCL between GPUs; PITTPACK_DIST_BACKEND=gloo runs the same ranks with
+        # host-staged collectives (ranks that share a GPU, e.g. to check this path)
+        backend = os.environ.get("PITTPACK_DIST_BACKEND", "nccl")
+        if backend == "nccl":
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local_rank))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     import pittpack_b200 as pp
     from pittpack_b200.poisson import pinned_empty
 
