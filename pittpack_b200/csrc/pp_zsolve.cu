@@ -31,7 +31,12 @@
 //   * eliminating each lane's first unknown leaves a P-row tridiagonal system
 //     in the lanes' last unknowns, solved by parallel cyclic reduction over
 //     warp shuffles (periodic systems through Sherman-Morrison); each lane
-//     then recovers its interior rows.
+//     then recovers its interior rows;
+//   * where every lane keeps exactly 16 or 32 rows in registers, they form two
+//     blocks of half that length whose sweeps run side by side (two
+//     independent FP64 recurrences per lane: the sweeps are bound by the
+//     latency of their dependent operations), and one more elimination step
+//     on the lane reduces the two blocks' rows to one before the shuffles.
 #include <type_traits>
 
 #include "pp_common.cuh"
@@ -145,6 +150,200 @@ PP_D void zt_each(int TS, int lts, int nz, int ts, F f)
     }
 }
 
+// The reduced system of a lane group, one row per lane L in the lanes' last
+// unknowns l:  ra l_{L-1} + rb l_L + rc l_{L+1} = rd,  lane indices wrapping
+// (periodic z; otherwise ra = 0 on the first lane and rc = 0 on the last).
+// Solved by parallel cyclic reduction over warp shuffles, the periodic one
+// through Sherman-Morrison; returns l_L.
+template <typename T>
+PP_D T zsolve_reduced(double ra, double rb, double rc, T rd, int lane, int P, bool periodic)
+{
+    if (P == 1)  // one row: its neighbours on both sides are itself
+        return zmul(1.0 / (ra + rb + rc), rd);
+    {
+        const double inv = 1.0 / rb;
+        ra *= inv;
+        rc *= inv;
+        rd = zmul(inv, rd);
+    }
+    double ru = 0.0, beta = 0.0;
+    const double gam = -1.0;
+    if (periodic) {
+        // the corners move into u v^T with u = (gam, 0, .., alpha),
+        // v = (1, 0, .., beta / gam): beta = a_0, alpha = c_{P-1}
+        beta = zshfl(ra, 0, P);
+        const double alpha = zshfl(rc, P - 1, P);
+        if (lane == 0) {
+            const double b0 = 1.0 - gam;
+            ra = 0.0;
+            rc /= b0;
+            rd = zmul(1.0 / b0, rd);
+            ru = gam / b0;
+        }
+        if (lane == P - 1) {
+            const double bl = 1.0 - alpha * beta / gam;
+            rc = 0.0;
+            ra /= bl;
+            rd = zmul(1.0 / bl, rd);
+            ru = alpha / bl;
+        }
+    }
+    for (int st = 1; st < P; st <<= 1) {
+        const bool hp = lane >= st, hn = lane + st < P;
+        double ap = zshfl_up(ra, st, P), cp = zshfl_up(rc, st, P);
+        T dp = zshfl_up(rd, st, P);
+        double an = zshfl_down(ra, st, P), cn = zshfl_down(rc, st, P);
+        T dnx = zshfl_down(rd, st, P);
+        if (!hp) {
+            ap = cp = 0.0;
+            dp = zzero<T>();
+        }
+        if (!hn) {
+            an = cn = 0.0;
+            dnx = zzero<T>();
+        }
+        const double inv = 1.0 / (1.0 - ra * cp - rc * an);
+        if (periodic) {
+            const double up = zshfl_up(ru, st, P), un = zshfl_down(ru, st, P);
+            ru = (ru - ra * (hp ? up : 0.0) - rc * (hn ? un : 0.0)) * inv;
+        }
+        rd = zmul(inv, zsub(zsub(rd, zmul(ra, dp)), zmul(rc, dnx)));
+        ra = -ra * ap * inv;
+        rc = -rc * cn * inv;
+    }
+    if (!periodic) return rd;
+    // fact = (y_0 + (beta/gam) y_{P-1}) / (1 + z_0 + (beta/gam) z_{P-1})
+    const double bg = beta / gam;
+    const T y0 = zshfl(rd, 0, P), yl = zshfl(rd, P - 1, P);
+    const double z0 = zshfl(ru, 0, P), zl = zshfl(ru, P - 1, P);
+    const T fact = zmul(1.0 / (1.0 + z0 + bg * zl), zadd(y0, zmul(bg, yl)));
+    return zsub(rd, zmul(ru, fact));
+}
+
+// The partition solve of one system by its lane group with each lane's MT
+// rows (registers xr, MT = nz / P) split into two blocks of H = MT / 2 rows,
+// A = xr[0, H) and B = xr[H, MT), whose sweeps run side by side (two
+// independent recurrences per lane instead of one of twice the length).
+// Every block is eliminated as in the one-block solve: forward sweep, spike
+// row of the block's first unknown f, its last row E1 -- leaving
+//   E0: f + e0a l_prev + e0c l = e0d,   E1: e1a f + l + e1c f_next = e1d
+// per block, l the block's last unknown and prev / next the adjacent blocks
+// (B of the previous lane, B of this lane for A; A of this lane, A of the
+// next lane for B).  Eliminating every f leaves one row per block in the l's;
+// eliminating l_A (its neighbours l_B of the previous lane and of this one)
+// leaves one row per lane in the l_B's, solved by zsolve_reduced; l_A, both
+// f's and the blocks' interior rows follow.  tab holds the interior pivots of
+// a block of H rows (gamma_i, alpha_i, i < H); d0 is row 0's right-hand side
+// (after the periodic zero-mode averaging); row 0 of the system is the first
+// row of A on lane 0 and row nz - 1 the last row of B on lane P - 1.
+template <int MT, typename T>
+PP_D void zsolve_split(T (&xr)[MT], const double2* tab, T d0, bool live, bool clear, int lane, int P,
+                       bool periodic, double lam, double A0, double B0, double C0, double AN, double BN,
+                       double CN)
+{
+    constexpr int H = MT / 2;
+    static_assert(H >= 4, "blocks of at least four rows");
+    const double* tg = reinterpret_cast<const double*>(tab);  // gamma_i = tg[2i], alpha_i = tg[2i+1]
+    const bool last = lane == P - 1;
+    // ---- forward sweeps of A and B ----------------------------------------------------
+    T dA = zzero<T>(), dB = zzero<T>();
+    double gA = 0.0, gB = 0.0, aA = 0.0, aB = 0.0;
+    if (live) {
+        bool lastB = false;
+#pragma unroll
+        for (int i = 1; i < H; ++i) {
+            const double ga = tg[2 * i];
+            const T nA = (i == 1) ? zmul(ga, xr[i]) : zmul(ga, zsub(xr[i], dA));
+            T nB;
+            if (i == H - 1 && last) {
+                // the system's last row closes B on the last lane
+                const double p = 1.0 / (BN - AN * gB);
+                aB = -AN * tg[2 * (i - 1) + 1] * p;
+                gB = CN * p;
+                nB = zmul(p, zsub(xr[H + i], zmul(AN, dB)));
+                lastB = true;
+            } else {
+                nB = (i == 1) ? zmul(ga, xr[H + i]) : zmul(ga, zsub(xr[H + i], dB));
+                gB = ga;
+            }
+            xr[i] = nA;
+            xr[H + i] = nB;
+            dA = nA;
+            dB = nB;
+            gA = ga;
+        }
+        aA = tg[2 * (H - 1) + 1];
+        if (!lastB) aB = aA;
+    }
+    // ---- backward sweeps: row 1 of a block in terms of its first and last unknowns
+    double br = 0.0, cr = 0.0;
+    T rA = zzero<T>(), rB = zzero<T>();
+    if (live) {
+        const double2 t2 = tab[H - 2];
+        br = t2.x;
+        cr = t2.y;
+        rA = xr[H - 2];
+        rB = xr[MT - 2];
+#pragma unroll
+        for (int i = H - 3; i >= 1; --i) {
+            const double g = tg[2 * i];
+            rA = zsub(xr[i], zmul(g, rA));
+            rB = zsub(xr[H + i], zmul(g, rB));
+        }
+    }
+    // ---- E0 of both blocks (A's first row is the system's row 0 on lane 0) -----------
+    const bool first = lane == 0;
+    const double a0 = first ? A0 : 1.0, b0 = first ? B0 : lam, c0 = first ? C0 : 1.0;
+    const double qA = 1.0 / (b0 - c0 * br);
+    const double e0aA = a0 * qA, e0cA = -c0 * cr * qA;
+    const T e0dA = zmul(qA, zsub(d0, zmul(c0, rA)));
+    const double qB = 1.0 / (lam - br);
+    const double e0aB = qB, e0cB = -cr * qB;
+    const T e0dB = zmul(qB, zsub(live ? xr[H] : zzero<T>(), rB));
+    // ---- rows of the blocks' last unknowns --------------------------------------------
+    // l_A:  raA l_B(prev lane) + rbA l_A + rcA l_B = rdA
+    const double raA = -aA * e0aA, rbA = 1.0 - aA * e0cA - gA * e0aB, rcA = -gA * e0cB;
+    const T rdA = zsub(zsub(dA, zmul(aA, e0dA)), zmul(gA, e0dB));
+    // l_B:  raB l_A + rbB l_B + rcB l_A(next lane) = rdB
+    const int nxt = (lane + 1) & (P - 1);
+    const double na0 = zshfl(e0aA, nxt, P), nc0 = zshfl(e0cA, nxt, P);
+    const T nd0 = zshfl(e0dA, nxt, P);
+    const double raB = -aB * e0aB, rbB = 1.0 - aB * e0cB - gB * na0, rcB = -gB * nc0;
+    const T rdB = zsub(zsub(dB, zmul(aB, e0dB)), zmul(gB, nd0));
+    // l_A = pd - pa l_B(prev lane) - pc l_B, substituted into the l_B rows
+    const double iA = 1.0 / rbA;
+    const double pa = raA * iA, pc = rcA * iA;
+    const T pd = zmul(iA, rdA);
+    const double npa = zshfl(pa, nxt, P), npc = zshfl(pc, nxt, P);
+    const T npd = zshfl(pd, nxt, P);
+    const T lB = zsolve_reduced(-raB * pa, rbB - raB * pc - rcB * npa, -rcB * npc,
+                                zsub(zsub(rdB, zmul(raB, pd)), zmul(rcB, npd)), lane, P, periodic);
+    const T lBp = zshfl(lB, (lane + P - 1) & (P - 1), P);
+    const T lA = zsub(zsub(pd, zmul(pa, lBp)), zmul(pc, lB));
+    const T fA = zsub(zsub(e0dA, zmul(e0aA, lBp)), zmul(e0cA, lA));
+    const T fB = zsub(zsub(e0dB, zmul(e0aB, lA)), zmul(e0cB, lB));
+    // ---- recover both blocks' rows ------------------------------------------------------
+    if (!live) return;
+    if (clear) {
+#pragma unroll
+        for (int i = 0; i < MT; ++i) xr[i] = zzero<T>();
+        return;
+    }
+    T xa = lA, xb = lB;
+    xr[H - 1] = lA;
+    xr[MT - 1] = lB;
+#pragma unroll
+    for (int i = H - 2; i >= 1; --i) {
+        const double2 ti = tab[i];
+        xa = zsub(zsub(xr[i], zmul(ti.y, fA)), zmul(ti.x, xa));
+        xb = zsub(zsub(xr[H + i], zmul(ti.y, fB)), zmul(ti.x, xb));
+        xr[i] = xa;
+        xr[H + i] = xb;
+    }
+    xr[0] = fA;
+    xr[H] = fB;
+}
+
 // shared-memory layout of one CTA
 struct ZLayout {
     int pitch;       // tile column pitch (elements)
@@ -197,7 +396,7 @@ struct ZTo32<double2> {
 // or at most MT (CAP = true, MT = 8, 12, 16, 24, 32: M = nz / P or one more,
 // the registers indexed statically under i < M guards); MT = 0: any nz, the
 // sweeps work on the tile in shared memory.
-template <bool CPLX, bool G32, int MT, bool CAP>
+template <bool CPLX, bool G32, int MT, bool CAP, bool SPLIT>
 __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
 {
     using T = typename std::conditional<CPLX, double2, double>::type;
@@ -257,13 +456,14 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     // recurrence straight into the table, marked by b_0 = 0.
     double* bsc = reinterpret_cast<double*>(zsm_raw + Lz.red_off);
     const int mm = Lz.mmax;
+    const int mcount = SPLIT ? MT / 2 : mm;  // entries built (split blocks: MT / 2 rows)
     for (int s = threadIdx.x; s < ts; s += blockDim.x) {
         const double lam = (-2.0 + a.ax[kx0 + s] * a.Cx) + a.ay[ky] * a.Cy;
         double* b = bsc + (size_t)s * mm;
-        if ((double)mm * log2(fabs(lam) + 1.0) < 900.0) {
+        if ((double)mcount * log2(fabs(lam) + 1.0) < 900.0) {
             double bm = 1.0, bc = lam;
             b[0] = 1.0;
-            for (int i = 1; i < mm; ++i) {
+            for (int i = 1; i < mcount; ++i) {
                 b[i] = bc;
                 const double bn = lam * bc - bm;
                 bm = bc;
@@ -272,7 +472,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         } else {
             double2* tb = reinterpret_cast<double2*>(zsm_raw + Lz.tab_off) + (size_t)s * mm;
             double gp = 0.0, ap = 0.0;
-            for (int i = 1; i < mm; ++i) {
+            for (int i = 1; i < mcount; ++i) {
                 const double p = (i == 1) ? 1.0 / lam : 1.0 / (lam - gp);
                 const double al = (i == 1) ? p : -ap * p;
                 tb[i] = make_double2(p, al);
@@ -291,7 +491,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         const int s = threadIdx.x >> ltp;
         const double* b = bsc + (size_t)s * mm;
         if (s < ts && b[0] != 0.0)
-            for (int i = (threadIdx.x & ((1 << ltp) - 1)) + 1; i < mm; i += 1 << ltp) {
+            for (int i = (threadIdx.x & ((1 << ltp) - 1)) + 1; i < mcount; i += 1 << ltp) {
                 const double inv = 1.0 / b[i];
                 reinterpret_cast<double2*>(zsm_raw + Lz.tab_off)[(size_t)s * mm + i] =
                     make_double2(b[i - 1] * inv, (i & 1) ? inv : -inv);
@@ -363,220 +563,164 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             CN = 0.0;
         }
 
-        // ---- forward sweep of the lane's block -------------------------------------
-        // row i (i >= 1) becomes alpha_i x_0 + x_i + gamma_i x_{i+1} = delta_i; delta
-        // overwrites the RHS in the tile (only this lane touches these rows)
-        double rA0 = 1.0, rB0 = lam, rC0 = 1.0;
-        if (s0 == 0) {
-            rA0 = A0;
-            rB0 = B0;
-            rC0 = C0;
-        }
-        T rD0 = zzero<T>(), dprev = zzero<T>();
-        // alpha of the block's last row: the table's, or the system's last row
-        double aprev = 0.0, gprev = 0.0;
-        bool last_special = false;
-        const double* tg = reinterpret_cast<const double*>(tab);  // gamma_i = tg[2i], alpha_i = tg[2i+1]
-        if (live) {
-            rD0 = X(0);
-            // the tile still holds every lane's input here (registers are
-            // written back at the end)
-            if (s0 == 0 && periodic && pin) rD0 = zmul(0.5, zadd(rD0, col[zpos(nz - 1)]));
-#pragma unroll
-            for (int i = 1; i < (MT > 0 ? MT : M); ++i) {
-                if (CAP && i >= M) break;
-                const int gk = s0 + i;
-                const T D = X(i);
-                double ga;
-                T dn;
-                // with MT rows per lane only the last unrolled row can be the
-                // system's last row: for real spectra the test is resolved at
-                // compile time elsewhere (for complex ones the register cost of
-                // the specialised code outweighs it).  Interior rows need gamma
-                // only; alpha matters for the block's last row alone.
-                if (!((MT == 0 || CAP || CPLX || i == MT - 1) && gk == nz - 1)) {
-                    ga = tg[2 * i];
-                    dn = (i == 1) ? zmul(ga, D) : zmul(ga, zsub(D, dprev));
-                } else if (i == 1) {
-                    const double inv = 1.0 / BN;
-                    aprev = AN * inv;
-                    ga = CN * inv;
-                    dn = zmul(inv, D);
-                    last_special = true;
-                } else {
-                    const double p = 1.0 / (BN - AN * gprev);
-                    aprev = -AN * tg[2 * (i - 1) + 1] * p;
-                    ga = CN * p;
-                    dn = zmul(p, zsub(D, zmul(AN, dprev)));
-                    last_special = true;
-                }
-                X(i) = dn;
-                gprev = ga;
-                dprev = dn;
+        if constexpr (SPLIT) {
+            static_assert(EXACT, "the split solve keeps exactly MT rows per lane");
+            T d0 = zzero<T>();
+            if (live) {
+                d0 = xr[0];
+                if (lane == 0 && periodic && pin) d0 = zmul(0.5, zadd(d0, col[zpos(nz - 1)]));
             }
-            if (!last_special) aprev = tg[2 * (M - 1) + 1];
-        }
-        // (alpha, gamma, delta) of the block's last row: the reduced row E1
-        const double e1a = aprev, e1c = gprev;
-        const T e1d = dprev;
-        __syncwarp(full);
-
-        // ---- backward sweep: row 1 in terms of x_0 and x_{M-1} ------------------------
-        // x_1 = dr - br x_0 - cr x_{M-1}.  The spikes are entries of the inverse
-        // of the block's interior matrix tridiag(1, lambda, 1) of order n = M-2:
-        // br = [T^-1]_11 = b_{n-1} / b_n = gamma_n and cr = [T^-1]_1n =
-        // (-1)^{n+1} / b_n = alpha_n, both in the table; only dr is swept.
-        double br = 0, cr = 0;
-        T dr = zzero<T>();
-        if (live && M >= 3) {
-            const double2 t2 = tab[M - 2];
-            br = t2.x;
-            cr = t2.y;
-            const double* tg = reinterpret_cast<const double*>(tab);
-            if constexpr (CAP) {
-                // registers indexed statically: rows above M - 2 are skipped
-#pragma unroll
-                for (int i = MT - 2; i >= 1; --i) {
-                    if (i > M - 2) continue;
-                    dr = (i == M - 2) ? X(i) : zsub(X(i), zmul(tg[2 * i], dr));
-                }
-            } else {
-                dr = X(M - 2);
-#pragma unroll
-                for (int i = M - 3; i >= 1; --i) dr = zsub(X(i), zmul(tg[2 * i], dr));
-            }
-        }
-        double e0a, e0c;
-        T e0d;
-        if (M == 2) {
-            const double inv = 1.0 / rB0;
-            e0a = rA0 * inv;
-            e0c = rC0 * inv;
-            e0d = zmul(inv, rD0);
+            zsolve_split<MT>(xr, tab, d0, live, zero && a.skip_zero, lane, P, periodic, lam, A0, B0, C0, AN, BN, CN);
         } else {
-            const double q = 1.0 / (rB0 - rC0 * br);
-            e0a = rA0 * q;
-            e0c = -rC0 * cr * q;
-            e0d = zmul(q, zsub(rD0, zmul(rC0, dr)));
-        }
+            // ---- forward sweep of the lane's block -------------------------------------
+            // row i (i >= 1) becomes alpha_i x_0 + x_i + gamma_i x_{i+1} = delta_i; delta
+            // overwrites the RHS in the tile (only this lane touches these rows)
+            double rA0 = 1.0, rB0 = lam, rC0 = 1.0;
+            if (s0 == 0) {
+                rA0 = A0;
+                rB0 = B0;
+                rC0 = C0;
+            }
+            T rD0 = zzero<T>(), dprev = zzero<T>();
+            // alpha of the block's last row: the table's, or the system's last row
+            double aprev = 0.0, gprev = 0.0;
+            bool last_special = false;
+            const double* tg = reinterpret_cast<const double*>(tab);  // gamma_i = tg[2i], alpha_i = tg[2i+1]
+            if (live) {
+                rD0 = X(0);
+                // the tile still holds every lane's input here (registers are
+                // written back at the end)
+                if (s0 == 0 && periodic && pin) rD0 = zmul(0.5, zadd(rD0, col[zpos(nz - 1)]));
+#pragma unroll
+                for (int i = 1; i < (MT > 0 ? MT : M); ++i) {
+                    if (CAP && i >= M) break;
+                    const int gk = s0 + i;
+                    const T D = X(i);
+                    double ga;
+                    T dn;
+                    // with MT rows per lane only the last unrolled row can be the
+                    // system's last row: for real spectra the test is resolved at
+                    // compile time elsewhere (for complex ones the register cost of
+                    // the specialised code outweighs it).  Interior rows need gamma
+                    // only; alpha matters for the block's last row alone.
+                    if (!((MT == 0 || CAP || CPLX || i == MT - 1) && gk == nz - 1)) {
+                        ga = tg[2 * i];
+                        dn = (i == 1) ? zmul(ga, D) : zmul(ga, zsub(D, dprev));
+                    } else if (i == 1) {
+                        const double inv = 1.0 / BN;
+                        aprev = AN * inv;
+                        ga = CN * inv;
+                        dn = zmul(inv, D);
+                        last_special = true;
+                    } else {
+                        const double p = 1.0 / (BN - AN * gprev);
+                        aprev = -AN * tg[2 * (i - 1) + 1] * p;
+                        ga = CN * p;
+                        dn = zmul(p, zsub(D, zmul(AN, dprev)));
+                        last_special = true;
+                    }
+                    X(i) = dn;
+                    gprev = ga;
+                    dprev = dn;
+                }
+                if (!last_special) aprev = tg[2 * (M - 1) + 1];
+            }
+            // (alpha, gamma, delta) of the block's last row: the reduced row E1
+            const double e1a = aprev, e1c = gprev;
+            const T e1d = dprev;
+            __syncwarp(full);
 
-        // ---- reduced system ---------------------------------------------------------------
-        // lane L's rows E0: f_L + e0a l_{L-1} + e0c l_L = e0d and
-        //                E1: e1a f_L + l_L + e1c f_{L+1} = e1d
-        // in its first (f) and last (l) unknowns.  Eliminating every f_L with E0
-        // leaves a tridiagonal system in l alone, one row per lane (the Schur
-        // complement, diagonally dominant with the original):
-        //   -e1a e0a l_{L-1} + (1 - e1a e0c - e1c e0a') l_L - e1c e0c' l_{L+1}
-        //       = e1d - e1a e0d - e1c e0d'          (' : lane L+1)
-        // The lane indices wrap (periodic z); without it e0a = 0 on the first lane
-        // and e1c = 0 on the last, so the wrapped values carry no weight.  It is
-        // solved by parallel cyclic reduction over warp shuffles, the periodic one
-        // through Sherman-Morrison, and f_L follows from E0.
-        const int nxt = (lane + 1) & (P - 1);
-        const double na0 = zshfl(e0a, nxt, P), nc0 = zshfl(e0c, nxt, P);
-        const T nd0 = zshfl(e0d, nxt, P);
-        double ra = -e1a * e0a;
-        const double rb = 1.0 - e1a * e0c - e1c * na0;
-        double rc = -e1c * nc0;
-        T rd = zsub(zsub(e1d, zmul(e1a, e0d)), zmul(e1c, nd0));
-        T xl;
-        if (P == 1) {
-            // one row: its neighbours on both sides are itself (zero without periodic z)
-            xl = zmul(1.0 / (ra + rb + rc), rd);
-        } else {
-            {
-                const double inv = 1.0 / rb;
-                ra *= inv;
-                rc *= inv;
-                rd = zmul(inv, rd);
-            }
-            double ru = 0.0, beta = 0.0;
-            const double gam = -1.0;
-            if (periodic) {
-                // the corners move into u v^T with u = (gam, 0, .., alpha),
-                // v = (1, 0, .., beta / gam): beta = a_0, alpha = c_{P-1}
-                beta = zshfl(ra, 0, P);
-                const double alpha = zshfl(rc, P - 1, P);
-                if (lane == 0) {
-                    const double b0 = 1.0 - gam;
-                    ra = 0.0;
-                    rc /= b0;
-                    rd = zmul(1.0 / b0, rd);
-                    ru = gam / b0;
-                }
-                if (lane == P - 1) {
-                    const double bl = 1.0 - alpha * beta / gam;
-                    rc = 0.0;
-                    ra /= bl;
-                    rd = zmul(1.0 / bl, rd);
-                    ru = alpha / bl;
-                }
-            }
-            for (int st = 1; st < P; st <<= 1) {
-                const bool hp = lane >= st, hn = lane + st < P;
-                double ap = zshfl_up(ra, st, P), cp = zshfl_up(rc, st, P);
-                T dp = zshfl_up(rd, st, P);
-                double an = zshfl_down(ra, st, P), cn = zshfl_down(rc, st, P);
-                T dnx = zshfl_down(rd, st, P);
-                if (!hp) {
-                    ap = cp = 0.0;
-                    dp = zzero<T>();
-                }
-                if (!hn) {
-                    an = cn = 0.0;
-                    dnx = zzero<T>();
-                }
-                const double inv = 1.0 / (1.0 - ra * cp - rc * an);
-                if (periodic) {
-                    const double up = zshfl_up(ru, st, P), un = zshfl_down(ru, st, P);
-                    ru = (ru - ra * (hp ? up : 0.0) - rc * (hn ? un : 0.0)) * inv;
-                }
-                rd = zmul(inv, zsub(zsub(rd, zmul(ra, dp)), zmul(rc, dnx)));
-                ra = -ra * ap * inv;
-                rc = -rc * cn * inv;
-            }
-            if (periodic) {
-                // fact = (y_0 + (beta/gam) y_{P-1}) / (1 + z_0 + (beta/gam) z_{P-1})
-                const double bg = beta / gam;
-                const T y0 = zshfl(rd, 0, P), yl = zshfl(rd, P - 1, P);
-                const double z0 = zshfl(ru, 0, P), zl = zshfl(ru, P - 1, P);
-                const T fact = zmul(1.0 / (1.0 + z0 + bg * zl), zadd(y0, zmul(bg, yl)));
-                xl = zsub(rd, zmul(ru, fact));
-            } else {
-                xl = rd;
-            }
-        }
-        const T xlp = zshfl(xl, (lane + P - 1) & (P - 1), P);
-        const T xf = zsub(zsub(e0d, zmul(e0a, xlp)), zmul(e0c, xl));
-        // ---- recover the block's rows ---------------------------------------------------
-        if (live && zero && a.skip_zero) {
-            // the kx = ky = 0 column is solved separately (in FP64 from plane sums)
+            // ---- backward sweep: row 1 in terms of x_0 and x_{M-1} ------------------------
+            // x_1 = dr - br x_0 - cr x_{M-1}.  The spikes are entries of the inverse
+            // of the block's interior matrix tridiag(1, lambda, 1) of order n = M-2:
+            // br = [T^-1]_11 = b_{n-1} / b_n = gamma_n and cr = [T^-1]_1n =
+            // (-1)^{n+1} / b_n = alpha_n, both in the table; only dr is swept.
+            double br = 0, cr = 0;
+            T dr = zzero<T>();
+            if (live && M >= 3) {
+                const double2 t2 = tab[M - 2];
+                br = t2.x;
+                cr = t2.y;
+                const double* tg = reinterpret_cast<const double*>(tab);
+                if constexpr (CAP) {
+                    // registers indexed statically: rows above M - 2 are skipped
 #pragma unroll
-            for (int i = 0; i < (MT > 0 ? MT : M); ++i) X(i) = zzero<T>();
-        } else if (live && CAP) {
-            T xn = xl;
-#pragma unroll
-            for (int i = MT - 1; i >= 1; --i) {
-                if (i > M - 1) continue;
-                if (i == M - 1) {
-                    X(i) = xl;
+                    for (int i = MT - 2; i >= 1; --i) {
+                        if (i > M - 2) continue;
+                        dr = (i == M - 2) ? X(i) : zsub(X(i), zmul(tg[2 * i], dr));
+                    }
                 } else {
+                    dr = X(M - 2);
+#pragma unroll
+                    for (int i = M - 3; i >= 1; --i) dr = zsub(X(i), zmul(tg[2 * i], dr));
+                }
+            }
+            double e0a, e0c;
+            T e0d;
+            if (M == 2) {
+                const double inv = 1.0 / rB0;
+                e0a = rA0 * inv;
+                e0c = rC0 * inv;
+                e0d = zmul(inv, rD0);
+            } else {
+                const double q = 1.0 / (rB0 - rC0 * br);
+                e0a = rA0 * q;
+                e0c = -rC0 * cr * q;
+                e0d = zmul(q, zsub(rD0, zmul(rC0, dr)));
+            }
+
+            // ---- reduced system ---------------------------------------------------------------
+            // lane L's rows E0: f_L + e0a l_{L-1} + e0c l_L = e0d and
+            //                E1: e1a f_L + l_L + e1c f_{L+1} = e1d
+            // in its first (f) and last (l) unknowns.  Eliminating every f_L with E0
+            // leaves a tridiagonal system in l alone, one row per lane (the Schur
+            // complement, diagonally dominant with the original):
+            //   -e1a e0a l_{L-1} + (1 - e1a e0c - e1c e0a') l_L - e1c e0c' l_{L+1}
+            //       = e1d - e1a e0d - e1c e0d'          (' : lane L+1)
+            // The lane indices wrap (periodic z); without it e0a = 0 on the first lane
+            // and e1c = 0 on the last, so the wrapped values carry no weight.  It is
+            // solved by parallel cyclic reduction over warp shuffles, the periodic one
+            // through Sherman-Morrison, and f_L follows from E0.
+            const int nxt = (lane + 1) & (P - 1);
+            const double na0 = zshfl(e0a, nxt, P), nc0 = zshfl(e0c, nxt, P);
+            const T nd0 = zshfl(e0d, nxt, P);
+            double ra = -e1a * e0a;
+            const double rb = 1.0 - e1a * e0c - e1c * na0;
+            double rc = -e1c * nc0;
+            T rd = zsub(zsub(e1d, zmul(e1a, e0d)), zmul(e1c, nd0));
+            const T xl = zsolve_reduced(ra, rb, rc, rd, lane, P, periodic);
+            const T xlp = zshfl(xl, (lane + P - 1) & (P - 1), P);
+            const T xf = zsub(zsub(e0d, zmul(e0a, xlp)), zmul(e0c, xl));
+            // ---- recover the block's rows ---------------------------------------------------
+            if (live && zero && a.skip_zero) {
+                // the kx = ky = 0 column is solved separately (in FP64 from plane sums)
+#pragma unroll
+                for (int i = 0; i < (MT > 0 ? MT : M); ++i) X(i) = zzero<T>();
+            } else if (live && CAP) {
+                T xn = xl;
+#pragma unroll
+                for (int i = MT - 1; i >= 1; --i) {
+                    if (i > M - 1) continue;
+                    if (i == M - 1) {
+                        X(i) = xl;
+                    } else {
+                        const double2 ti = tab[i];
+                        xn = zsub(zsub(X(i), zmul(ti.y, xf)), zmul(ti.x, xn));
+                        X(i) = xn;
+                    }
+                }
+                X(0) = xf;
+            } else if (live) {
+                T xn = xl;
+                X(M - 1) = xl;
+#pragma unroll
+                for (int i = M - 2; i >= 1; --i) {
                     const double2 ti = tab[i];
                     xn = zsub(zsub(X(i), zmul(ti.y, xf)), zmul(ti.x, xn));
                     X(i) = xn;
                 }
+                X(0) = xf;
             }
-            X(0) = xf;
-        } else if (live) {
-            T xn = xl;
-            X(M - 1) = xl;
-#pragma unroll
-            for (int i = M - 2; i >= 1; --i) {
-                const double2 ti = tab[i];
-                xn = zsub(zsub(X(i), zmul(ti.y, xf)), zmul(ti.x, xn));
-                X(i) = xn;
-            }
-            X(0) = xf;
         }
         if constexpr (EXACT) {
             if (live) {
@@ -703,9 +847,10 @@ cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
         if (cplx) cap = rmax <= 8 ? 8 : rmax <= 12 ? 12 : rmax <= 16 ? 16 : 0;
         else cap = rmax <= 8 ? 8 : rmax <= 16 ? 16 : rmax <= 24 ? 24 : rmax <= 32 ? 32 : 0;
     }
-#define PP_ZL(C, G, M, K)                                                                                       \
+#define PP_ZL(C, G, M, K) PP_ZLK(C, G, M, K, false)
+#define PP_ZLK(C, G, M, K, S)                                                                                   \
     do {                                                                                                        \
-        auto kfn = zsolve_kernel<C, G, M, K>;                                                                   \
+        auto kfn = zsolve_kernel<C, G, M, K, S>;                                                                \
         if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) \
             return e;                                                                                           \
         kfn<<<grid, block, smem, st>>>(a);                                                                      \
@@ -713,8 +858,8 @@ cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
 #define PP_ZLM(C, G)                                  \
     do {                                              \
         if (mt == 8) PP_ZL(C, G, 8, false);           \
-        else if (mt == 16) PP_ZL(C, G, 16, false);    \
-        else if (mt == 32 && !C) PP_ZL(C, G, 32, false); \
+        else if (mt == 16) PP_ZLK(C, G, 16, false, true); \
+        else if (mt == 32 && !C) PP_ZLK(C, G, 32, false, true); \
         else if (cap == 8) PP_ZL(C, G, 8, true);      \
         else if (cap == 12 && C) PP_ZL(C, G, 12, true);  \
         else if (cap == 16) PP_ZL(C, G, 16, true);    \
@@ -728,5 +873,6 @@ cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
     else PP_ZLM(false, false);
 #undef PP_ZLM
 #undef PP_ZL
+#undef PP_ZLK
     return cudaGetLastError();
 }
