@@ -60,3 +60,58 @@ PP_D C c_scale(C a, typename CReal<C>::type s) { return mkc<C>(a.x * s, a.y * s)
 // multiply by SIGN * i
 template <int SIGN, typename C>
 PP_D C c_mul_si(C a) { return SIGN > 0 ? mkc<C>(-a.y, a.x) : mkc<C>(a.y, -a.x); }
+
+// ---- bulk-copy staging (the copy engine, not the LSU pipe) --------------------------
+PP_D unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// mbarrier with one arrival, armed for 'bytes' of bulk copies
+PP_D void mbar_init(unsigned bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+PP_D void mbar_expect(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+// global -> shared bulk copy (both addresses 16-byte aligned, bytes a
+// multiple of 16), completion counted on the mbarrier
+PP_D void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+// wait for phase 0 of the mbarrier, at most 'limit' polls; true if it completed
+PP_D bool mbar_wait0(unsigned bar, long limit)
+{
+    for (long i = 0; i < limit; ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// shared -> global bulk copy (both addresses 16-byte aligned, bytes a
+// multiple of 16) in the thread's bulk async-group
+PP_D void bulk_s2g(void* dst, const void* src, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+// close the thread's bulk async-group and wait until its copies have read
+// their shared-memory sources (the writes to global memory complete on their own)
+PP_D void bulk_commit_wait_read()
+{
+    asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+}
+// this thread's shared-memory writes made visible to later bulk copies
+PP_D void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }

@@ -141,6 +141,7 @@ struct PPZArgs {
     int skip_zero;      // write zeros for the kx = ky = 0 column
     int tiled;          // spectrum in the z-tiled layout: tile (ky, kx / TS) is the
                         // contiguous block [k][kx % TS] at (ky (nx / TS) + kx / TS) nz TS
+    int* err;           // counts CTAs whose bounded waits ran out (may be null)
 };
 
 // lanes that share one z system (a power of two <= 32)

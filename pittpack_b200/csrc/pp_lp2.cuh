@@ -123,42 +123,7 @@ PP_D void cp_async(void* smem, const void* gmem)
     if (BYTES == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 
-// ---- bulk-copy staging (the copy engine, not the LSU pipe) --------------------------
-PP_D unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-// mbarrier with one arrival, armed for 'bytes' of bulk copies
-PP_D void mbar_init(unsigned bar)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-}
-PP_D void mbar_expect(unsigned bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
-// global -> shared bulk copy (both addresses 16-byte aligned, bytes a
-// multiple of 16), completion counted on the mbarrier
-PP_D void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-// wait for phase 0 of the mbarrier, at most 'limit' polls; true if it completed
-PP_D bool mbar_wait0(unsigned bar, long limit)
-{
-    for (long i = 0; i < limit; ++i) {
-        unsigned done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(bar)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
+// bulk-copy staging: smem_u32, mbar_*, bulk_g2s (pp_common.cuh)
 
 // row pitch (elements) of the strided pass's raw tile [element][line]: the
 // smallest pitch above the tile's line count whose rows start on 16-byte

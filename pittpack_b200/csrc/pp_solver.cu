@@ -823,6 +823,7 @@ int launch_solve(pp_solver_s* h, int stages = STAGE_ALL, const StageZ* sz = null
     pp_zsolve_config_p(znz, s_cplx, ncol, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile, zny);
     z.P = h->tune.zsolve_lanes;
     z.tiled = zt ? 1 : 0;
+    z.err = h->errc.as<int>();
     z.tiles_x = (ncol + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
     z.ay = h->ty.eig.as<double>() + (sz ? sz->j0 : 0);
@@ -1009,6 +1010,7 @@ int launch_mixed(pp_solver_s* h)
     pp_zsolve_config_p(nz, s_cplx, ncol, h->tune.zsolve_lanes, &z.TS, &zthreads, zt ? zt : h->tune.zsolve_tile, ny);
     z.P = h->tune.zsolve_lanes;
     z.tiled = zt ? 1 : 0;
+    z.err = h->errc.as<int>();
     z.tiles_x = (ncol + z.TS - 1) / z.TS;
     z.ax = h->tx.eig.as<double>();
     z.ay = h->ty.eig.as<double>();

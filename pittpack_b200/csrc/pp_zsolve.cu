@@ -419,6 +419,19 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     // or the z-tiled one, where this CTA's tile is one contiguous block
     const long plane = a.tiled ? (long)a.TS : (long)nx * ny;
     const long col0 = a.tiled ? (long)blockIdx.x * nz * a.TS : (long)ky * nx + kx0;
+    // z-tiled with exactly MT rows per lane: each lane block of the tile (MT
+    // rows x TS systems, contiguous in global memory) moves as one bulk copy
+    // (the copy engine, not the LSU pipe) into a chunk of shared memory, the
+    // chunks 16 bytes apart so that the lanes of a phase read distinct banks
+    // (or two-way shared ones at one system per half warp); the tile goes back
+    // the same way
+    const int cbytes = SPLIT ? MT * a.TS * (int)sizeof(T) : 0;  // one lane block
+    const int cpitch = cbytes + 16;
+    const bool bulk = SPLIT && !G32 && a.tiled && ts == a.TS && P * MT == nz &&
+                      (size_t)P * cpitch <= Lz.tab_off && (reinterpret_cast<uintptr_t>(a.data) & 15) == 0;
+    __shared__ __align__(8) unsigned long long zbar;
+    const unsigned bar = smem_u32(&zbar);
+    unsigned char* gtile = reinterpret_cast<unsigned char*>(g + col0);
 
     // ---- load the tile asynchronously (thread -> (system, row) without division:
     //      TS is a power of two) and build the pivot tables while it lands ------------
@@ -437,7 +450,14 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
                 }
             }
         }
-        if (!G32)
+        if (bulk) {
+            if (threadIdx.x == 0) {
+                mbar_init(bar);
+                mbar_expect(bar, (unsigned)(P * cbytes));
+                for (int c = 0; c < P; ++c)
+                    bulk_g2s(zsm_raw + (size_t)c * cpitch, gtile + (size_t)c * cbytes, (unsigned)cbytes, bar);
+            }
+        } else if (!G32)
             zt_each<T>(a.TS, lts, nz, ts, [&](int s2, int k) {
                 if (sizeof(T) == 16) cp_async16(&tile[s2 * Lz.pitch + zpos(k)], &g[k * plane + col0 + s2]);
                 else cp_async8(&tile[s2 * Lz.pitch + zpos(k)], &g[k * plane + col0 + s2]);
@@ -498,7 +518,17 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             }
     }
     cp_async_wait_all();
-    __syncthreads();
+    if (bulk) {
+        // a bounded wait (about a second of polls): a CTA whose copies never
+        // land counts itself and leaves without output, with every thread
+        const bool landed = mbar_wait0(bar, 1L << 22);
+        if (__syncthreads_or(!landed)) {
+            if (threadIdx.x == 0 && a.err) atomicAdd(a.err, 1);
+            return;
+        }
+    } else {
+        __syncthreads();
+    }
     if (G32) {
         const T32* stg = reinterpret_cast<const T32*>(zsm_raw + Lz.stg_off);
         const int s = threadIdx.x & (a.TS - 1);
@@ -534,9 +564,16 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         // with MT a power of two >= 8 and s0 = lane MT, zpos(s0 + i) = zpos(s0) + zpos(i)
         T xr[MT > 0 ? MT : 1];
         T* xcol = col + zpos(s0);
+        // (bulk) the lane's rows of system s in its chunk, TS apart
+        T* lrow = reinterpret_cast<T*>(zsm_raw + (size_t)lane * cpitch) + (live ? s : 0);
         if constexpr (EXACT) {
+            if (bulk) {
 #pragma unroll
-            for (int i = 0; i < MT; ++i) xr[i] = live ? xcol[zpos(i)] : zzero<T>();
+                for (int i = 0; i < MT; ++i) xr[i] = live ? lrow[i * a.TS] : zzero<T>();
+            } else {
+#pragma unroll
+                for (int i = 0; i < MT; ++i) xr[i] = live ? xcol[zpos(i)] : zzero<T>();
+            }
         } else if constexpr (MT > 0) {
 #pragma unroll
             for (int i = 0; i < MT; ++i) xr[i] = (live && i < M) ? col[zpos(s0 + i)] : zzero<T>();
@@ -568,7 +605,11 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             T d0 = zzero<T>();
             if (live) {
                 d0 = xr[0];
-                if (lane == 0 && periodic && pin) d0 = zmul(0.5, zadd(d0, col[zpos(nz - 1)]));
+                if (lane == 0 && periodic && pin) {
+                    const T last = bulk ? reinterpret_cast<const T*>(zsm_raw + (size_t)(P - 1) * cpitch)[(MT - 1) * a.TS + s]
+                                        : col[zpos(nz - 1)];
+                    d0 = zmul(0.5, zadd(d0, last));
+                }
             }
             zsolve_split<MT>(xr, tab, d0, live, zero && a.skip_zero, lane, P, periodic, lam, A0, B0, C0, AN, BN, CN);
         } else {
@@ -723,7 +764,10 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             }
         }
         if constexpr (EXACT) {
-            if (live) {
+            if (live && bulk) {
+#pragma unroll
+                for (int i = 0; i < MT; ++i) lrow[i * a.TS] = xr[i];
+            } else if (live) {
 #pragma unroll
                 for (int i = 0; i < MT; ++i) xcol[zpos(i)] = xr[i];
             }
@@ -736,9 +780,15 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         }
         __syncwarp(full);
     }
+    if (bulk) fence_proxy_async_smem();  // the rows written above, read by the bulk copies
     __syncthreads();
 
-    if (G32) {
+    if (bulk) {
+        if (threadIdx.x == 0) {
+            for (int c = 0; c < P; ++c) bulk_s2g(gtile + (size_t)c * cbytes, zsm_raw + (size_t)c * cpitch, (unsigned)cbytes);
+            bulk_commit_wait_read();
+        }
+    } else if (G32) {
         const int s = threadIdx.x & (a.TS - 1);
         const int kstep = blockDim.x >> lts;
         if (s < ts)
