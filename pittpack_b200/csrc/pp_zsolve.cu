@@ -388,6 +388,18 @@ struct ZTo32<double2> {
     static PP_D double2 up(float2 v) { return make_double2(v.x, v.y); }
     static PP_D float2 down(double2 v) { return make_float2((float)v.x, (float)v.y); }
 };
+// a stored element (FP64, or FP32 for the refined solve's spectra) to and from
+// the FP64 arithmetic type T
+template <typename T>
+PP_D T zup(T v) { return v; }
+template <typename T>
+PP_D T zup(typename ZTo32<T>::type v) { return ZTo32<T>::up(v); }
+template <typename TG, typename T>
+PP_D TG zdown(T v)
+{
+    if constexpr (std::is_same<TG, T>::value) return v;
+    else return ZTo32<T>::down(v);
+}
 
 // G32: the spectrum in global memory is FP32 (refined mixed-precision solve);
 // the tile and all arithmetic stay FP64.  MT > 0: every lane keeps its rows
@@ -424,14 +436,16 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     // (the copy engine, not the LSU pipe) into a chunk of shared memory, the
     // chunks 16 bytes apart so that the lanes of a phase read distinct banks
     // (or two-way shared ones at one system per half warp); the tile goes back
-    // the same way
-    const int cbytes = SPLIT ? MT * a.TS * (int)sizeof(T) : 0;  // one lane block
+    // the same way.  FP32 spectra (G32) stay FP32 in the chunks: the lanes
+    // convert their rows on the way into and out of registers
+    using TG = typename std::conditional<G32, T32, T>::type;  // element in global memory
+    const int cbytes = SPLIT ? MT * a.TS * (int)sizeof(TG) : 0;  // one lane block
     const int cpitch = cbytes + 16;
-    const bool bulk = SPLIT && !G32 && a.tiled && ts == a.TS && P * MT == nz &&
+    const bool bulk = SPLIT && a.tiled && ts == a.TS && P * MT == nz &&
                       (size_t)P * cpitch <= Lz.tab_off && (reinterpret_cast<uintptr_t>(a.data) & 15) == 0;
     __shared__ __align__(8) unsigned long long zbar;
     const unsigned bar = smem_u32(&zbar);
-    unsigned char* gtile = reinterpret_cast<unsigned char*>(g + col0);
+    unsigned char* gtile = G32 ? reinterpret_cast<unsigned char*>(g32 + col0) : reinterpret_cast<unsigned char*>(g + col0);
 
     // ---- load the tile asynchronously (thread -> (system, row) without division:
     //      TS is a power of two) and build the pivot tables while it lands ------------
@@ -439,7 +453,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     {
         const int s = threadIdx.x & (a.TS - 1);
         const int kstep = blockDim.x >> lts;
-        if (s < ts) {
+        if (s < ts && !bulk) {
             if (G32) {
                 // FP32 elements copied asynchronously into the staging area;
                 // converted to the FP64 tile once they have landed
@@ -529,7 +543,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
     } else {
         __syncthreads();
     }
-    if (G32) {
+    if (G32 && !bulk) {
         const T32* stg = reinterpret_cast<const T32*>(zsm_raw + Lz.stg_off);
         const int s = threadIdx.x & (a.TS - 1);
         const int kstep = blockDim.x >> lts;
@@ -565,11 +579,11 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         T xr[MT > 0 ? MT : 1];
         T* xcol = col + zpos(s0);
         // (bulk) the lane's rows of system s in its chunk, TS apart
-        T* lrow = reinterpret_cast<T*>(zsm_raw + (size_t)lane * cpitch) + (live ? s : 0);
+        TG* lrow = reinterpret_cast<TG*>(zsm_raw + (size_t)lane * cpitch) + (live ? s : 0);
         if constexpr (EXACT) {
             if (bulk) {
 #pragma unroll
-                for (int i = 0; i < MT; ++i) xr[i] = live ? lrow[i * a.TS] : zzero<T>();
+                for (int i = 0; i < MT; ++i) xr[i] = live ? zup<T>(lrow[i * a.TS]) : zzero<T>();
             } else {
 #pragma unroll
                 for (int i = 0; i < MT; ++i) xr[i] = live ? xcol[zpos(i)] : zzero<T>();
@@ -606,7 +620,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
             if (live) {
                 d0 = xr[0];
                 if (lane == 0 && periodic && pin) {
-                    const T last = bulk ? reinterpret_cast<const T*>(zsm_raw + (size_t)(P - 1) * cpitch)[(MT - 1) * a.TS + s]
+                    const T last = bulk ? zup<T>(reinterpret_cast<const TG*>(zsm_raw + (size_t)(P - 1) * cpitch)[(MT - 1) * a.TS + s])
                                         : col[zpos(nz - 1)];
                     d0 = zmul(0.5, zadd(d0, last));
                 }
@@ -766,7 +780,7 @@ __global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
         if constexpr (EXACT) {
             if (live && bulk) {
 #pragma unroll
-                for (int i = 0; i < MT; ++i) lrow[i * a.TS] = xr[i];
+                for (int i = 0; i < MT; ++i) lrow[i * a.TS] = zdown<TG>(xr[i]);
             } else if (live) {
 #pragma unroll
                 for (int i = 0; i < MT; ++i) xcol[zpos(i)] = xr[i];
