@@ -408,8 +408,15 @@ PP_D TG zdown(T v)
 // or at most MT (CAP = true, MT = 8, 12, 16, 24, 32: M = nz / P or one more,
 // the registers indexed statically under i < M guards); MT = 0: any nz, the
 // sweeps work on the tile in shared memory.
+// The split kernels are held to 128 registers (two CTAs of 256 threads, or
+// four of 128, per SM): their sweeps are bound by the latency of dependent
+// FP64 operations, and the extra resident warps outweigh a few spilled values
+// (512^3: real 32 rows per lane 0.436 -> 0.380 ms with 92 bytes spilled,
+// complex 16 rows 0.446 -> 0.381 ms; FP32 complex spectra 0.37 -> 0.33 ms).
+// Not the FP32 real spectra, whose conversions make the cap cost more than
+// it gains (0.33 -> 0.36 ms).
 template <bool CPLX, bool G32, int MT, bool CAP, bool SPLIT>
-__global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
+__global__ void __launch_bounds__(PP_Z_THREADS, (SPLIT && (CPLX || !G32)) ? 2 : 1) zsolve_kernel(PPZArgs a)
 {
     using T = typename std::conditional<CPLX, double2, double>::type;
     using T32 = typename ZTo32<T>::type;
@@ -919,16 +926,18 @@ cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
             return e;                                                                                           \
         kfn<<<grid, block, smem, st>>>(a);                                                                      \
     } while (0)
+// (the row counts a complex or real launch never takes are replaced by ones
+// it does, so that no dead instance is compiled)
 #define PP_ZLM(C, G)                                  \
     do {                                              \
         if (mt == 8) PP_ZL(C, G, 8, false);           \
         else if (mt == 16) PP_ZLK(C, G, 16, false, true); \
-        else if (mt == 32 && !C) PP_ZLK(C, G, 32, false, true); \
+        else if (mt == 32 && !C) PP_ZLK(C, G, (C ? 16 : 32), false, true); \
         else if (cap == 8) PP_ZL(C, G, 8, true);      \
-        else if (cap == 12 && C) PP_ZL(C, G, 12, true);  \
+        else if (cap == 12 && C) PP_ZL(C, G, (C ? 12 : 16), true); \
         else if (cap == 16) PP_ZL(C, G, 16, true);    \
-        else if (cap == 24 && !C) PP_ZL(C, G, 24, true); \
-        else if (cap == 32 && !C) PP_ZL(C, G, 32, true); \
+        else if (cap == 24 && !C) PP_ZL(C, G, (C ? 16 : 24), true); \
+        else if (cap == 32 && !C) PP_ZL(C, G, (C ? 16 : 32), true); \
         else PP_ZL(C, G, 0, false);                   \
     } while (0)
     if (cplx && a.data_fp32) PP_ZLM(true, true);
