@@ -408,15 +408,8 @@ PP_D TG zdown(T v)
 // or at most MT (CAP = true, MT = 8, 12, 16, 24, 32: M = nz / P or one more,
 // the registers indexed statically under i < M guards); MT = 0: any nz, the
 // sweeps work on the tile in shared memory.
-// The split kernels are held to 128 registers (two CTAs of 256 threads, or
-// four of 128, per SM): their sweeps are bound by the latency of dependent
-// FP64 operations, and the extra resident warps outweigh a few spilled values
-// (512^3: real 32 rows per lane 0.436 -> 0.380 ms with 92 bytes spilled,
-// complex 16 rows 0.446 -> 0.381 ms; FP32 complex spectra 0.37 -> 0.33 ms).
-// Not the FP32 real spectra, whose conversions make the cap cost more than
-// it gains (0.33 -> 0.36 ms).
 template <bool CPLX, bool G32, int MT, bool CAP, bool SPLIT>
-__global__ void __launch_bounds__(PP_Z_THREADS, (SPLIT && (CPLX || !G32)) ? 2 : 1) zsolve_kernel(PPZArgs a)
+PP_D void zsolve_body(PPZArgs a)
 {
     using T = typename std::conditional<CPLX, double2, double>::type;
     using T32 = typename ZTo32<T>::type;
@@ -438,17 +431,22 @@ __global__ void __launch_bounds__(PP_Z_THREADS, (SPLIT && (CPLX || !G32)) ? 2 : 
     // or the z-tiled one, where this CTA's tile is one contiguous block
     const long plane = a.tiled ? (long)a.TS : (long)nx * ny;
     const long col0 = a.tiled ? (long)blockIdx.x * nz * a.TS : (long)ky * nx + kx0;
-    // z-tiled with exactly MT rows per lane: each lane block of the tile (MT
-    // rows x TS systems, contiguous in global memory) moves as one bulk copy
-    // (the copy engine, not the LSU pipe) into a chunk of shared memory, the
-    // chunks 16 bytes apart so that the lanes of a phase read distinct banks
-    // (or two-way shared ones at one system per half warp); the tile goes back
-    // the same way.  FP32 spectra (G32) stay FP32 in the chunks: the lanes
-    // convert their rows on the way into and out of registers
+    // z-tiled with the rows in registers (two half blocks per lane, or any
+    // row count for complex spectra: 384^3 complex 0.30 -> 0.28 ms, where real
+    // ones lose 3 %): each lane block of the tile (the
+    // lane's rows x TS systems, contiguous in global memory) moves as one bulk
+    // copy (the copy engine, not the LSU pipe) into a chunk of shared memory,
+    // the chunks 16 bytes past the longest block so that the lanes of a phase
+    // read distinct banks (or two-way shared ones at one system per half
+    // warp); the tile goes back the same way.  FP32 spectra (G32) stay FP32 in
+    // the chunks: the lanes convert their rows on the way into and out of
+    // registers.  Lane L's block is rows L brows + min(L, brem) on, brows + 1
+    // of them for the first brem lanes, brows for the rest.
     using TG = typename std::conditional<G32, T32, T>::type;  // element in global memory
-    const int cbytes = SPLIT ? MT * a.TS * (int)sizeof(TG) : 0;  // one lane block
-    const int cpitch = cbytes + 16;
-    const bool bulk = SPLIT && a.tiled && ts == a.TS && P * MT == nz &&
+    const int brows = SPLIT ? MT : nz / P, brem = SPLIT ? 0 : nz - brows * P;  // split: nz = P MT
+    const int crow = a.TS * (int)sizeof(TG);                  // bytes of one tile row
+    const int cpitch = (brows + (brem ? 1 : 0)) * crow + 16;
+    const bool bulk = (SPLIT || (CAP && CPLX)) && a.tiled && ts == a.TS && crow % 16 == 0 &&
                       (size_t)P * cpitch <= Lz.tab_off && (reinterpret_cast<uintptr_t>(a.data) & 15) == 0;
     __shared__ __align__(8) unsigned long long zbar;
     const unsigned bar = smem_u32(&zbar);
@@ -474,9 +472,10 @@ __global__ void __launch_bounds__(PP_Z_THREADS, (SPLIT && (CPLX || !G32)) ? 2 : 
         if (bulk) {
             if (threadIdx.x == 0) {
                 mbar_init(bar);
-                mbar_expect(bar, (unsigned)(P * cbytes));
+                mbar_expect(bar, (unsigned)(nz * crow));
                 for (int c = 0; c < P; ++c)
-                    bulk_g2s(zsm_raw + (size_t)c * cpitch, gtile + (size_t)c * cbytes, (unsigned)cbytes, bar);
+                    bulk_g2s(zsm_raw + (size_t)c * cpitch, gtile + (size_t)(c * brows + min(c, brem)) * crow,
+                             (unsigned)((brows + (c < brem ? 1 : 0)) * crow), bar);
             }
         } else if (!G32)
             zt_each<T>(a.TS, lts, nz, ts, [&](int s2, int k) {
@@ -597,7 +596,8 @@ __global__ void __launch_bounds__(PP_Z_THREADS, (SPLIT && (CPLX || !G32)) ? 2 : 
             }
         } else if constexpr (MT > 0) {
 #pragma unroll
-            for (int i = 0; i < MT; ++i) xr[i] = (live && i < M) ? col[zpos(s0 + i)] : zzero<T>();
+            for (int i = 0; i < MT; ++i)
+                xr[i] = (live && i < M) ? (bulk ? zup<T>(lrow[i * a.TS]) : col[zpos(s0 + i)]) : zzero<T>();
         }
         auto X = [&](int i) -> T& {
             if constexpr (MT > 0) return xr[i];
@@ -652,7 +652,12 @@ __global__ void __launch_bounds__(PP_Z_THREADS, (SPLIT && (CPLX || !G32)) ? 2 : 
                 rD0 = X(0);
                 // the tile still holds every lane's input here (registers are
                 // written back at the end)
-                if (s0 == 0 && periodic && pin) rD0 = zmul(0.5, zadd(rD0, col[zpos(nz - 1)]));
+                if (s0 == 0 && periodic && pin) {
+                    // row nz - 1: the last of lane P - 1's brows rows
+                    const T last = bulk ? zup<T>(reinterpret_cast<const TG*>(zsm_raw + (size_t)(P - 1) * cpitch)[(brows - 1) * a.TS + s])
+                                        : col[zpos(nz - 1)];
+                    rD0 = zmul(0.5, zadd(rD0, last));
+                }
 #pragma unroll
                 for (int i = 1; i < (MT > 0 ? MT : M); ++i) {
                     if (CAP && i >= M) break;
@@ -795,8 +800,11 @@ __global__ void __launch_bounds__(PP_Z_THREADS, (SPLIT && (CPLX || !G32)) ? 2 : 
         } else if constexpr (MT > 0) {
             if (live) {
 #pragma unroll
-                for (int i = 0; i < MT; ++i)
-                    if (i < M) col[zpos(s0 + i)] = xr[i];
+                for (int i = 0; i < MT; ++i) {
+                    if (i >= M) continue;
+                    if (bulk) lrow[i * a.TS] = zdown<TG>(xr[i]);
+                    else col[zpos(s0 + i)] = xr[i];
+                }
             }
         }
         __syncwarp(full);
@@ -806,7 +814,9 @@ __global__ void __launch_bounds__(PP_Z_THREADS, (SPLIT && (CPLX || !G32)) ? 2 : 
 
     if (bulk) {
         if (threadIdx.x == 0) {
-            for (int c = 0; c < P; ++c) bulk_s2g(gtile + (size_t)c * cbytes, zsm_raw + (size_t)c * cpitch, (unsigned)cbytes);
+            for (int c = 0; c < P; ++c)
+                bulk_s2g(gtile + (size_t)(c * brows + min(c, brem)) * crow, zsm_raw + (size_t)c * cpitch,
+                         (unsigned)((brows + (c < brem ? 1 : 0)) * crow));
             bulk_commit_wait_read();
         }
     } else if (G32) {
@@ -819,6 +829,33 @@ __global__ void __launch_bounds__(PP_Z_THREADS, (SPLIT && (CPLX || !G32)) ? 2 : 
         zt_each<T>(a.TS, lts, nz, ts, [&](int s2, int k) { g[k * plane + col0 + s2] = tile[s2 * Lz.pitch + zpos(k)]; });
 }
 
+
+template <bool CPLX, bool G32, int MT, bool CAP, bool SPLIT>
+__global__ void __launch_bounds__(PP_Z_THREADS) zsolve_kernel(PPZArgs a)
+{
+    zsolve_body<CPLX, G32, MT, CAP, SPLIT>(a);
+}
+// The split kernels held to 128 registers (two CTAs of 256 threads, or four
+// of 128, per SM): their sweeps are bound by the latency of dependent FP64
+// operations, and the extra resident warps outweigh a few spilled values
+// (512^3: real 32 rows per lane 0.436 -> 0.380 ms with 92 bytes spilled,
+// complex 16 rows 0.446 -> 0.381 ms; FP32 complex spectra 0.37 -> 0.33 ms).
+// Not for FP32 real spectra, whose conversions make the cap cost more than
+// it gains (0.33 -> 0.36 ms).  A separate kernel: naming a minimum of one
+// CTA per SM in the other kernels' launch bounds lets the compiler spend
+// more registers on them than the one-argument form does.
+template <bool CPLX, bool G32, int MT>
+__global__ void __launch_bounds__(PP_Z_THREADS, 2) zsolve_split_r128_kernel(PPZArgs a)
+{
+    zsolve_body<CPLX, G32, MT, false, true>(a);
+}
+// the split kernel a launch takes (only that one is compiled)
+template <bool CPLX, bool G32, int MT>
+void (*split_kernel())(PPZArgs)
+{
+    if constexpr (CPLX || !G32) return zsolve_split_r128_kernel<CPLX, G32, MT>;
+    else return zsolve_kernel<CPLX, G32, MT, false, true>;
+}
 }  // namespace
 
 int pp_zsolve_lanes(int nz, bool cplx, bool large)
@@ -918,10 +955,14 @@ cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
         if (cplx) cap = rmax <= 8 ? 8 : rmax <= 12 ? 12 : rmax <= 16 ? 16 : 0;
         else cap = rmax <= 8 ? 8 : rmax <= 16 ? 16 : rmax <= 24 ? 24 : rmax <= 32 ? 32 : 0;
     }
-#define PP_ZL(C, G, M, K) PP_ZLK(C, G, M, K, false)
+#define PP_ZL(C, G, M, K) PP_ZLF((zsolve_kernel<C, G, M, K, false>))
 #define PP_ZLK(C, G, M, K, S)                                                                                   \
     do {                                                                                                        \
-        auto kfn = zsolve_kernel<C, G, M, K, S>;                                                                \
+        PP_ZLF((split_kernel<C, G, M>()));                                                                     \
+    } while (0)
+#define PP_ZLF(KFN)                                                                                             \
+    do {                                                                                                        \
+        auto kfn = KFN;                                                                                         \
         if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) \
             return e;                                                                                           \
         kfn<<<grid, block, smem, st>>>(a);                                                                      \
@@ -947,5 +988,6 @@ cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
 #undef PP_ZLM
 #undef PP_ZL
 #undef PP_ZLK
+#undef PP_ZLF
     return cudaGetLastError();
 }
