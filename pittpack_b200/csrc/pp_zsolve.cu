@@ -16,8 +16,11 @@
 //
 // B200 layout and algorithm:
 //   * a CTA owns TS adjacent kx columns of one ky row; it reads the TS x nz
-//     tile with coalesced row segments into shared memory (rows skewed by one
-//     slot every 16 to spread banks), solves, and writes the tile back;
+//     tile into shared memory, solves, and writes the tile back: in the
+//     z-tiled layout (the tile one contiguous block) with one bulk copy per
+//     lane's block of rows where the rows live in registers, else with
+//     coalesced row segments (rows skewed by one slot every 16 to spread
+//     banks);
 //   * a group of P lanes (P = 32 / systems per warp) solves one system by the
 //     partition method: lane L owns a contiguous block of M ~ nz/P rows and
 //     eliminates it so that every interior unknown is expressed through the
@@ -402,12 +405,14 @@ PP_D TG zdown(T v)
 }
 
 // G32: the spectrum in global memory is FP32 (refined mixed-precision solve);
-// the tile and all arithmetic stay FP64.  MT > 0: every lane keeps its rows
+// all arithmetic stays FP64 (the shared tile too, except in the bulk-copied
+// chunks, which hold the stored elements).  MT > 0: every lane keeps its rows
 // in registers through the three sweeps, reading and writing its rows of the
 // tile once -- exactly MT rows each (CAP = false, nz = P MT, MT = 8, 16, 32),
 // or at most MT (CAP = true, MT = 8, 12, 16, 24, 32: M = nz / P or one more,
 // the registers indexed statically under i < M guards); MT = 0: any nz, the
-// sweeps work on the tile in shared memory.
+// sweeps work on the tile in shared memory.  SPLIT: exactly MT = 16 or 32
+// rows per lane, swept as two half blocks (zsolve_split).
 template <bool CPLX, bool G32, int MT, bool CAP, bool SPLIT>
 PP_D void zsolve_body(PPZArgs a)
 {
