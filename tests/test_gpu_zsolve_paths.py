@@ -46,6 +46,7 @@ FP64_CASES = [
     (256, 256, 64, "NNNNPP"),   # real, 2 lanes x 32 rows, periodic z with the zero mode
     (256, 256, 64, "DDDDPP"),   # real, split, periodic z without a zero mode
     (256, 256, 48, "NDNDDD"),   # real, 2 lanes x 24 rows: uneven register rows
+    (256, 256, 1024, "NNNNDD"), # real, 32 lanes x 32 rows: split, 256-thread CTAs, chunks near the tile's size
     (512, 256, 32, "PPPPDD"),   # complex half spectra, 2 lanes x 16 rows: split, bulk tiles
     (512, 256, 32, "PPPPPP"),   # complex, split, periodic z with the zero mode
     (512, 256, 24, "PPPPPP"),   # complex, 2 lanes x 12 rows: uneven rows, bulk tiles, zero mode
