@@ -21,12 +21,16 @@ def _singular(bc):
     return bc[0:2] in ("NN", "PP") and bc[2:4] in ("NN", "PP") and bc[4] in "NP" and bc[5] in "NP"
 
 
-def _solve(nx, ny, nz, bc, f, **opts):
+def _solve(nx, ny, nz, bc, f, zsolve_tile=0, **opts):
     import pittpack_b200 as pp
 
     with pp.make_Poisson(nx, ny, nz) as M:
         M.assignBoundary(bc)
         M.setOptions(**opts)
+        if zsolve_tile:
+            # a z tile other than the y pass's lines per tile: the usual
+            # [k][ky][kx] spectrum, tiles copied element by element
+            M.setTuning(zsolve_tile=zsolve_tile)
         M.assignRhs(f)
         M.pittPack()
         P = M.getSolution()
@@ -45,11 +49,12 @@ FP64_CASES = [
     (256, 256, 32, "NNNNDD"),   # real, 1 lane x 32 rows: split, bulk tiles
     (256, 256, 64, "NNNNPP"),   # real, 2 lanes x 32 rows, periodic z with the zero mode
     (256, 256, 64, "DDDDPP"),   # real, split, periodic z without a zero mode
-    (256, 256, 48, "NDNDDD"),   # real, 2 lanes x 24 rows: uneven register rows
+    (256, 256, 48, "NDNDDD"),   # real, 2 lanes x 24 rows: split
+    (256, 256, 40, "NDNDDD"),   # real, 2 lanes x 20 rows: uneven register rows
     (256, 256, 1024, "NNNNDD"), # real, 32 lanes x 32 rows: split, 256-thread CTAs, chunks near the tile's size
     (512, 256, 32, "PPPPDD"),   # complex half spectra, 2 lanes x 16 rows: split, bulk tiles
     (512, 256, 32, "PPPPPP"),   # complex, split, periodic z with the zero mode
-    (512, 256, 24, "PPPPPP"),   # complex, 2 lanes x 12 rows: uneven rows, bulk tiles, zero mode
+    (512, 256, 24, "PPPPPP"),   # complex, 2 lanes x 12 rows: split, bulk tiles, zero mode
     (512, 256, 40, "PPPPNN"),   # complex, 4 lanes x 10 rows: uneven rows, bulk tiles
 ]
 
@@ -59,6 +64,18 @@ def test_fp64_register_paths_vs_oracle(nx, ny, nz, bc):
     f = _rhs(nx, ny, nz, bc, nx + ny + nz)
     Q = O.solve(O.problem(nx, ny, nz, bc), f)
     P = _solve(nx, ny, nz, bc, f)
+    assert O.rel_l2(P, Q) <= 1e-12
+
+
+@pytest.mark.parametrize("nx,ny,nz,bc", [(256, 256, 48, "NDNDDD"), (256, 256, 64, "NNNNPP"),
+                                         (512, 256, 24, "PPPPPP"), (512, 256, 32, "PPPPDD")])
+def test_fp64_register_paths_untiled_vs_oracle(nx, ny, nz, bc):
+    """The same register paths on the usual spectrum layout (a z tile of one
+    system, which the z-tiled layout never has): rows read from and written to
+    the skewed shared column."""
+    f = _rhs(nx, ny, nz, bc, nx + ny + nz + 1)
+    Q = O.solve(O.problem(nx, ny, nz, bc), f)
+    P = _solve(nx, ny, nz, bc, f, zsolve_tile=1)
     assert O.rel_l2(P, Q) <= 1e-12
 
 
