@@ -35,7 +35,7 @@
 //     in the lanes' last unknowns, solved by parallel cyclic reduction over
 //     warp shuffles (periodic systems through Sherman-Morrison); each lane
 //     then recovers its interior rows;
-//   * where every lane keeps exactly 12, 16, 24 or 32 rows in registers, they form two
+//   * where every lane keeps exactly 10, 12, 16, 20, 24 or 32 rows in registers, they form two
 //     blocks of half that length whose sweeps run side by side (two
 //     independent FP64 recurrences per lane: the sweeps are bound by the
 //     latency of their dependent operations), and one more elimination step
@@ -408,10 +408,10 @@ PP_D TG zdown(T v)
 // all arithmetic stays FP64 (the shared tile too, except in the bulk-copied
 // chunks, which hold the stored elements).  MT > 0: every lane keeps its rows
 // in registers through the three sweeps, reading and writing its rows of the
-// tile once -- exactly MT rows each (CAP = false, nz = P MT, MT = 8, 12, 16, 24, 32),
+// tile once -- exactly MT rows each (CAP = false, nz = P MT, MT = 8, 10, 12, 16, 20, 24, 32),
 // or at most MT (CAP = true, MT = 8, 12, 16, 24, 32: M = nz / P or one more,
 // the registers indexed statically under i < M guards); MT = 0: any nz, the
-// sweeps work on the tile in shared memory.  SPLIT: exactly MT = 12, 16, 24 or 32
+// sweeps work on the tile in shared memory.  SPLIT: exactly MT = 10, 12, 16, 20, 24 or 32
 // rows per lane, swept as two half blocks (zsolve_split).
 template <bool CPLX, bool G32, int MT, bool CAP, bool SPLIT>
 PP_D void zsolve_body(PPZArgs a)
@@ -587,8 +587,8 @@ PP_D void zsolve_body(PPZArgs a)
         const double2* tab = reinterpret_cast<const double2*>(zsm_raw + Lz.tab_off) + (size_t)(live ? s : 0) * Lz.mmax;
         // the lane's rows: registers (MT > 0) or the tile column
         // with MT a power of two >= 8 and s0 = lane MT, zpos(s0 + i) = zpos(s0) + zpos(i)
-        // (s0 + i never crosses a multiple of 16 that s0 does not); 12 and 24
-        // rows index the skewed column directly
+        // (s0 + i never crosses a multiple of 16 that s0 does not); 10, 12, 20
+        // and 24 rows index the skewed column directly
         constexpr bool ZP2 = (MT & (MT - 1)) == 0;
         T xr[MT > 0 ? MT : 1];
         T* xcol = col + zpos(s0);
@@ -965,8 +965,8 @@ cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
     // rows per lane fixed at compile time where every lane has the same count;
     // else the smallest register capacity that holds every lane's rows
     const int rows = a.nz / a.P, rmax = (a.nz + a.P - 1) / a.P;
-    const int mt = (a.nz % a.P == 0 && (rows == 8 || rows == 16 || (rows == 12 && cplx) || (rows == 24 && !cplx) ||
-                                        (rows == 32 && !cplx))) ? rows : 0;
+    const int mt = (a.nz % a.P == 0 && (rows == 8 || rows == 16 || ((rows == 10 || rows == 12) && cplx) ||
+                                        ((rows == 20 || rows == 24 || rows == 32) && !cplx))) ? rows : 0;
     int cap = 0;
     if (!mt && large) {
         if (cplx) cap = rmax <= 8 ? 8 : rmax <= 12 ? 12 : rmax <= 16 ? 16 : 0;
@@ -993,6 +993,8 @@ cudaError_t pp_launch_zsolve(const PPZArgs& a0, bool cplx, cudaStream_t st)
         else if (mt == 32 && !C) PP_ZLK(C, G, (C ? 16 : 32), false, true); \
         else if (mt == 24 && !C) PP_ZLK(C, G, (C ? 16 : 24), false, true); \
         else if (mt == 12 && C) PP_ZLK(C, G, (C ? 12 : 16), false, true); \
+        else if (mt == 20 && !C) PP_ZLK(C, G, (C ? 16 : 20), false, true); \
+        else if (mt == 10 && C) PP_ZLK(C, G, (C ? 10 : 16), false, true); \
         else if (cap == 8) PP_ZL(C, G, 8, true);      \
         else if (cap == 12 && C) PP_ZL(C, G, (C ? 12 : 16), true); \
         else if (cap == 16) PP_ZL(C, G, 16, true);    \

@@ -50,12 +50,14 @@ FP64_CASES = [
     (256, 256, 64, "NNNNPP"),   # real, 2 lanes x 32 rows, periodic z with the zero mode
     (256, 256, 64, "DDDDPP"),   # real, split, periodic z without a zero mode
     (256, 256, 48, "NDNDDD"),   # real, 2 lanes x 24 rows: split
-    (256, 256, 40, "NDNDDD"),   # real, 2 lanes x 20 rows: uneven register rows
+    (256, 256, 40, "NDNDDD"),   # real, 2 lanes x 20 rows: split
+    (256, 256, 36, "NNNNDD"),   # real, 2 lanes x 18 rows: uneven register rows
     (256, 256, 1024, "NNNNDD"), # real, 32 lanes x 32 rows: split, 256-thread CTAs, chunks near the tile's size
     (512, 256, 32, "PPPPDD"),   # complex half spectra, 2 lanes x 16 rows: split, bulk tiles
     (512, 256, 32, "PPPPPP"),   # complex, split, periodic z with the zero mode
     (512, 256, 24, "PPPPPP"),   # complex, 2 lanes x 12 rows: split, bulk tiles, zero mode
-    (512, 256, 40, "PPPPNN"),   # complex, 4 lanes x 10 rows: uneven rows, bulk tiles
+    (512, 256, 40, "PPPPNN"),   # complex, 4 lanes x 10 rows: split, bulk tiles
+    (512, 256, 36, "PPPPNN"),   # complex, 4 lanes x 9 rows: uneven rows, bulk tiles
 ]
 
 
@@ -67,8 +69,8 @@ def test_fp64_register_paths_vs_oracle(nx, ny, nz, bc):
     assert O.rel_l2(P, Q) <= 1e-12
 
 
-@pytest.mark.parametrize("nx,ny,nz,bc", [(256, 256, 48, "NDNDDD"), (256, 256, 64, "NNNNPP"),
-                                         (512, 256, 24, "PPPPPP"), (512, 256, 32, "PPPPDD")])
+@pytest.mark.parametrize("nx,ny,nz,bc", [(256, 256, 48, "NDNDDD"), (256, 256, 64, "NNNNPP"), (256, 256, 40, "DDDDNN"),
+                                         (512, 256, 24, "PPPPPP"), (512, 256, 32, "PPPPDD"), (512, 256, 40, "PPPPDD")])
 def test_fp64_register_paths_untiled_vs_oracle(nx, ny, nz, bc):
     """The same register paths on the usual spectrum layout (a z tile of one
     system, which the z-tiled layout never has): rows read from and written to
