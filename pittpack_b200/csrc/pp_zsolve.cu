@@ -436,11 +436,12 @@ PP_D void zsolve_body(PPZArgs a)
     // or the z-tiled one, where this CTA's tile is one contiguous block
     const long plane = a.tiled ? (long)a.TS : (long)nx * ny;
     const long col0 = a.tiled ? (long)blockIdx.x * nz * a.TS : (long)ky * nx + kx0;
-    // z-tiled with the rows in registers (two half blocks per lane, or any
-    // row count for complex spectra: 384^3 complex 0.30 -> 0.28 ms, where real
-    // ones lose 3 %): each lane block of the tile (the
-    // lane's rows x TS systems, contiguous in global memory) moves as one bulk
-    // copy (the copy engine, not the LSU pipe) into a chunk of shared memory,
+    // Bulk-copied tiles: z-tiled, rows in registers, and either the split
+    // kernels or complex spectra with uneven row counts (where complex uneven
+    // rows gained 0.30 -> 0.28 ms at 384^3, real ones lost 3 %).  Each lane
+    // block of the tile (the lane's rows x TS systems, contiguous in global
+    // memory) moves as one bulk copy (the copy engine, not the LSU pipe) into a
+    // chunk of shared memory,
     // the chunks 16 bytes past the longest block so that the lanes of a phase
     // read distinct banks (or two-way shared ones at one system per half
     // warp); the tile goes back the same way.  FP32 spectra (G32) stay FP32 in
